@@ -1,0 +1,421 @@
+#!/usr/bin/env python3
+"""Benchmark of the lsCOMP uint16 codec on B200 (one JSON line on rank 0).
+
+Workload: the CSSI-like stack, 600 x 1813 x 1558 uint16 (3.39 GB, z fastest,
+seeded synthetic data).  One step = compress + decompress in the lossless
+mode (-b 1 1 1 1 -p 1) and compress + decompress lossy (-b 3 5 10 15 -p 0.5):
+four passes over the stack.
+
+    value  = 4 * input bytes per step / device time of the step (GB/s, 1e9),
+             inputs resident in HBM, CUDA events on the launching stream;
+    e2e    = the same metric through the C ABI with host buffers: every pass
+             copies its input from pinned host memory and its result back;
+    roofline  = the dominant kernel's algorithmic bytes per launch / its mean
+             launch time, against MEASURED_PEAKS.json hbm_gbs;
+    cpu_baseline = the C/OpenMP oracle on a bounded frame sample, all cores.
+
+--impl reference times the reference's own CUDA build (oracle/_ref) through
+its host API on the same stack and steps.  --gpus N (torchrun) runs N
+independent replicas, one per GPU: the codec does not shard, so there is no
+data-path collective; the step time is the max over ranks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "sc25-lscomp_b200"))
+
+DIMS = (600, 1813, 1558)
+MODES = [("lossless", (1, 1, 1, 1), 1.0), ("lossy", (3, 5, 10, 15), 0.5)]
+SEED = 2
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--dims", type=str, default=None, help="x,y,z (default: the CSSI-like stack)")
+    ap.add_argument("--kind", default="cssi", choices=["cssi", "xpcs", "small"])
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_stack(kind, dims):
+    import lscomp
+
+    return getattr(lscomp, f"synth_{kind}")(dims, seed=SEED if kind == "cssi" else 1)
+
+
+def cpu_baseline(kind, dims, budget_s):
+    """Oracle (C/OpenMP port of the reference algorithm) on the first frames
+    of the same stack, all host threads, lossless + lossy compress/decompress."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import lscomp
+    from oracle import Oracle
+
+    orc = Oracle()
+    threads = orc.max_threads()
+    x, y, z = dims
+
+    def run(nf):
+        d = (nf, y, z)
+        a = getattr(lscomp, f"synth_{kind}")(dims, seed=SEED if kind == "cssi" else 1, frames=(0, nf))
+        t0 = time.perf_counter()
+        for _, bins, p in MODES:
+            s, _ = orc.compress(a, d, bins, p, threads=threads)
+            orc.decompress(s, d, bins, p, threads=threads)
+        return time.perf_counter() - t0, a.size * 2
+
+    nf = 2
+    t, nbytes = run(nf)
+    target = max(1, min(x, int(nf * budget_s / max(t, 1e-3))))
+    if target > nf:
+        nf = target
+        t, nbytes = run(nf)
+    return {"value": round(4 * nbytes / t / 1e9, 4), "unit": "GB/s", "cores": threads, "kind": "port",
+            "sample": f"first {nf} of {x} frames ({nbytes / 1e9:.3f} GB), lossless+lossy compress+decompress, "
+                      f"{t:.1f} s"}
+
+
+def dist_init(n):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return rank, world, local
+
+
+def max_over_ranks(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def main():
+    args = parse()
+    dims = tuple(int(v) for v in args.dims.split(",")) if args.dims else DIMS
+    rank, world, local = dist_init(args.gpus)
+    import torch
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    nbytes = dims[0] * dims[1] * dims[2] * 2
+    hbm, peak_kind = peaks()
+    stream = torch.cuda.current_stream()
+    h = make_stack(args.kind, dims)
+    d_in = torch.from_numpy(h.view(np.int16)).to(dev)
+    cap = (lambda nb: (nb + 3) // 4 * 4 + 128 * nb)(dims[0] * ((dims[1] + 7) // 8) * ((dims[2] + 7) // 8))
+    d_cmp = torch.zeros(cap, dtype=torch.uint8, device=dev)
+    d_dec = torch.empty_like(d_in)
+    config = {"workload": f"{args.kind}-like stack {dims[0]}x{dims[1]}x{dims[2]} uint16, z fastest",
+              "modes": "lossless -b 1 1 1 1 -p 1; lossy -b 3 5 10 15 -p 0.5",
+              "step": "compress+decompress in both modes (4 passes)",
+              "input_bytes": nbytes, "l2": "inputs (3.39 GB) larger than L2 (126 MB); no flush needed",
+              "parallelism": f"replicas{world}"}
+
+    if args.impl == "reference":
+        return bench_reference(args, dims, rank, world, dev, d_in, d_cmp, d_dec, nbytes, config, h)
+
+    import lscomp
+
+    ws = lscomp.Workspace(local)
+    sizes = {}
+
+    def step(ev=None):
+        for i, (name, bins, p) in enumerate(MODES):
+            if ev is not None:
+                ev[4 * i].record(stream)
+            lscomp.compress_async(ws, d_in, dims, bins, p, d_cmp)
+            if ev is not None:
+                ev[4 * i + 1].record(stream)
+            lscomp.decompress_async(ws, d_cmp, sizes[name], dims, bins, p, d_dec)
+            if ev is not None:
+                ev[4 * i + 2].record(stream)
+
+    # exact stream lengths (and a correctness check) before timing
+    for name, bins, p in MODES:
+        sl, rs = lscomp.compress_into(ws, d_in, dims, bins, p, d_cmp)
+        sizes[name] = sl
+        sizes[name + "_ref_size"] = rs
+        lscomp.decompress_into(ws, d_cmp, sl, dims, bins, p, d_dec)
+        if name == "lossless" and not torch.equal(d_dec, d_in):
+            raise SystemExit("lossless round trip failed")
+    for _ in range(max(args.warmup, 3)):
+        step()
+    ws.check()
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(8)] for _ in range(args.steps)]
+    e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(local)
+    launches0 = lscomp.launch_count()
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    e_start.record(stream)
+    for k in range(args.steps):
+        step(evs[k])
+    e_end.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    launches = lscomp.launch_count() - launches0
+    ws.check()
+    total_ms = max_over_ranks(e_start.elapsed_time(e_end), world)
+    ms_step = total_ms / args.steps
+    per = {}
+    for i, (name, bins, p) in enumerate(MODES):
+        tc = float(np.mean([e[4 * i].elapsed_time(e[4 * i + 1]) for e in evs]))
+        td = float(np.mean([e[4 * i + 1].elapsed_time(e[4 * i + 2]) for e in evs]))
+        sl = sizes[name]
+        per[name] = {"compress_gbs": round(nbytes / tc / 1e6, 1), "decompress_gbs": round(nbytes / td / 1e6, 1),
+                     "compress_ms": round(tc, 4), "decompress_ms": round(td, 4), "stream_bytes": sl,
+                     "ratio": round(nbytes / sizes[name + "_ref_size"], 4),
+                     "compress_hbm_frac": round((nbytes + sl) / tc / 1e6 / hbm, 4),
+                     "decompress_hbm_frac": round((nbytes + sl) / td / 1e6 / hbm, 4)}
+    # dominant kernel: largest time share in the step
+    shares = []
+    for name, _, _ in MODES:
+        shares.append((per[name]["compress_ms"], f"enc_kernel ({name})", nbytes + sizes[name]))
+        shares.append((per[name]["decompress_ms"], f"dec_kernel ({name})", nbytes + sizes[name]))
+    shares.sort(reverse=True)
+    t_dom, k_dom, b_dom = shares[0]
+    achieved = b_dom / t_dom / 1e6
+    roofline = {"bound": "hbm", "kernel": k_dom, "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                "frac": round(achieved / hbm, 4), "peak_kind": peak_kind,
+                "traffic": None, "algorithmic_bytes_per_launch": b_dom}
+    prof = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(prof):
+        try:
+            tr = json.load(open(prof)).get(k_dom)
+            if tr:
+                roofline["traffic"] = tr
+        except Exception:
+            pass
+    value = world * 4 * nbytes / (ms_step / 1e3) / 1e9
+
+    e2e = bench_e2e(args, dims, ws, h, dev, nbytes, sizes, world)
+    out = {"metric": "lsCOMP compress+decompress throughput (lossless and lossy b=3 5 10 15 p=0.5), "
+                     "uncompressed GB per second",
+           "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+           "warmup": max(args.warmup, 3), "ms_per_step": round(ms_step, 4), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic (seeded CSSI-like generator)",
+           "config": config, "per_mode": per, "roofline": roofline, "e2e": e2e, "gpu_launches": int(launches),
+           "clocks": clk}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(args.kind, dims, args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def bench_e2e(args, dims, ws, h, dev, nbytes, sizes, world):
+    """Host buffers in, host buffers out, through the C ABI: per mode the input
+    goes host->device, compress, the stream device->host; the stream goes
+    host->device, decompress, the stack device->host."""
+    import torch
+
+    import lscomp
+
+    h_in = torch.from_numpy(h.view(np.int16)).pin_memory()
+    h_out = torch.empty_like(h_in).pin_memory()
+    cap = max(sizes[m[0]] for m in MODES)
+    h_cmp = torch.empty(cap, dtype=torch.uint8).pin_memory()
+    d_in = torch.empty(h_in.numel(), dtype=torch.int16, device=dev)
+    d_cmp = torch.empty(lscomp.max_stream_bytes(dims), dtype=torch.uint8, device=dev)
+    d_dec = torch.empty_like(d_in)
+    stream = torch.cuda.current_stream()
+    h2d = d2h = 0
+
+    def step():
+        nonlocal h2d, d2h
+        h2d = d2h = 0
+        for name, bins, p in MODES:
+            d_in.copy_(h_in, non_blocking=True)
+            sl, _ = lscomp.compress_into(ws, d_in, dims, bins, p, d_cmp)
+            h_cmp[:sl].copy_(d_cmp[:sl], non_blocking=True)
+            d_cmp[:sl].copy_(h_cmp[:sl], non_blocking=True)
+            lscomp.decompress_into(ws, d_cmp, sl, dims, bins, p, d_dec)
+            h_out.copy_(d_dec, non_blocking=True)
+            h2d += nbytes + sl
+            d2h += sl + nbytes
+        torch.cuda.synchronize()
+
+    step()
+    if not torch.equal(h_out, h_in) and MODES[-1][0] == "lossless":
+        raise SystemExit("e2e round trip failed")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), world) / args.e2e_steps
+    return {"value": round(world * 4 * nbytes / (ms / 1e3) / 1e9, 2), "unit": "GB/s",
+            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "ms_per_step": round(ms, 3),
+            "path": "lscomp_compress_u16 / lscomp_decompress_u16 (C ABI), pinned host buffers"}
+
+
+def bench_reference(args, dims, rank, world, dev, d_in, d_cmp, d_dec, nbytes, config, h):
+    """The reference's own CUDA build through its host API
+    (cuLSZ_compression_uint16_bsize64 / cuLSZ_decompression_uint16_bsize64),
+    timed like the reference CLI times it: the whole host call."""
+    import torch
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    if world > 1 and rank != 0:
+        # the reference arm runs on rank 0 only
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+        return
+    try:
+        from oracle import REF_LIB, RefLib
+
+        ref = RefLib(REF_LIB)
+    except Exception as e:  # the reference build is not present
+        print(json.dumps({"impl": "reference", "unavailable": f"reference build missing: {e}"}))
+        return
+    sizes = {}
+    for name, bins, p in MODES:
+        d_cmp.zero_()
+        sizes[name] = ref.compress(d_in.data_ptr(), d_cmp.data_ptr(), dims, bins, p)
+        torch.cuda.synchronize()
+
+    def step():
+        for name, bins, p in MODES:
+            ref.compress(d_in.data_ptr(), d_cmp.data_ptr(), dims, bins, p)
+            ref.decompress(d_dec.data_ptr(), d_cmp.data_ptr(), sizes[name], dims, bins, p)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    value = 4 * nbytes / (ms / 1e3) / 1e9
+    out = {"impl": "reference",
+           "metric": "lsCOMP compress+decompress throughput (lossless and lossy b=3 5 10 15 p=0.5), "
+                     "uncompressed GB per second",
+           "value": round(value, 2), "unit": "GB/s", "n_gpus": 1, "steps": args.steps,
+           "warmup": max(args.warmup, 3), "ms_per_step": round(ms, 4), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic (seeded CSSI-like generator)",
+           "config": config, "clocks": clk,
+           "cpu_baseline": {"value": round(value, 2), "unit": "GB/s", "cores": 1, "kind": "reference",
+                            "sample": "the reference's CUDA sources (nvcc -O3 sm_100a) through its host API on the "
+                                      "full stack; the reference has no CPU implementation"},
+           "e2e": {"value": round(value, 2), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

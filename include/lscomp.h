@@ -1,0 +1,100 @@
+/*
+ * lscomp.h -- C ABI of the B200-native lsCOMP codec (uint16 detector stacks).
+ *
+ * Plain C: pointers, sizes, an opaque workspace and a CUDA stream passed as
+ * void*.  All data pointers are device pointers unless stated otherwise.
+ * Every entry point returns an lscomp_status.
+ *
+ * Stream format (unchanged from the reference, lsCOMP/src/cuLSZ_kernel.cu):
+ *   [nb header bytes][zero pad to a multiple of 4][payload blocks in block order]
+ * with nb = X * ceil(Y/8) * ceil(Z/8) blocks of 8x8 values (z fastest).
+ * Header byte = pool << 7 | bin_choice << 5 | rate.
+ *
+ * Entry points and the reference interface each replaces:
+ *   lscomp_compress_u16 / _async     cuLSZ_compression_uint16_bsize64
+ *                                    (lsCOMP/include/cuLSZ_entry.h:10,
+ *                                     lsCOMP/src/cuLSZ_entry.cu:93-131)
+ *   lscomp_decompress_u16 / _async   cuLSZ_decompression_uint16_bsize64
+ *                                    (lsCOMP/include/cuLSZ_entry.h:11,
+ *                                     lsCOMP/src/cuLSZ_entry.cu:133-166)
+ *   lscomp_workspace_*               the per-call cudaMalloc/cudaMemset/cudaFree
+ *                                    of the scan scratch (cuLSZ_entry.cu:105-114,
+ *                                    128-130), made reusable
+ */
+#ifndef LSCOMP_H
+#define LSCOMP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    LSCOMP_OK = 0,
+    LSCOMP_ERR_ARG = 1,      /* bad dimension, bin, pointer alignment or size */
+    LSCOMP_ERR_CAPACITY = 2, /* output (or readable input) too small for the stream */
+    LSCOMP_ERR_CUDA = 3,     /* a CUDA runtime call failed */
+    LSCOMP_ERR_TIMEOUT = 4,  /* a bounded wait inside a kernel ran out */
+    LSCOMP_ERR_CORRUPT = 5,  /* stream inconsistent with the given geometry */
+    LSCOMP_ERR_RANGE = 6,    /* values the stream format cannot represent */
+    LSCOMP_ERR_NOMEM = 7     /* device or host allocation failed */
+} lscomp_status;
+
+typedef struct lscomp_workspace lscomp_workspace;
+
+/* library version, e.g. 100 for 0.1.0 */
+int lscomp_version(void);
+const char *lscomp_status_string(int status);
+
+/* number of 8x8 blocks of an X x Y x Z stack */
+uint64_t lscomp_block_count(uint32_t x, uint32_t y, uint32_t z);
+/* worst-case stream length for uint16 data: roundup4(nb) + 128 * nb */
+uint64_t lscomp_max_stream_bytes_u16(uint32_t x, uint32_t y, uint32_t z);
+
+/* A workspace holds the scan state of one stream of calls (about 8 bytes
+   per tile) on one device.  Calls that share a workspace must be ordered
+   (same CUDA stream, or synchronised).  device < 0 means the current device. */
+int lscomp_workspace_create(lscomp_workspace **ws, int device);
+int lscomp_workspace_destroy(lscomp_workspace *ws);
+
+/* Compress.  d_in: X*Y*Z uint16 (2-byte aligned).  bins: four bins > 0.
+   pooling: the -p threshold (a block pools iff (float)zeros/64 > pooling).
+   d_out: cap bytes.  On success *stream_len = bytes of the stream and
+   *ref_size = payload + nb, the value the reference's host API reports
+   (either pointer may be NULL).  Synchronises the stream. */
+int lscomp_compress_u16(lscomp_workspace *ws, const uint16_t *d_in, uint32_t x, uint32_t y, uint32_t z,
+                        const uint32_t bins[4], float pooling, uint8_t *d_out, uint64_t cap,
+                        uint64_t *stream_len, uint64_t *ref_size, void *stream);
+
+/* Same work without any host synchronisation: {stream_len, payload bytes}
+   are written to d_sizes[0..1] (device memory, may be NULL) when the kernel
+   finishes; errors are read later with lscomp_workspace_check. */
+int lscomp_compress_u16_async(lscomp_workspace *ws, const uint16_t *d_in, uint32_t x, uint32_t y,
+                              uint32_t z, const uint32_t bins[4], float pooling, uint8_t *d_out,
+                              uint64_t cap, uint64_t *d_sizes, void *stream);
+
+/* Decompress.  d_in: stream, cmp_len readable bytes (the stream length, or
+   more).  Writes every element of d_out (X*Y*Z uint16), zero for blocks of
+   rate 0.  Synchronises the stream. */
+int lscomp_decompress_u16(lscomp_workspace *ws, const uint8_t *d_in, uint64_t cmp_len, uint32_t x,
+                          uint32_t y, uint32_t z, const uint32_t bins[4], float pooling, uint16_t *d_out,
+                          void *stream);
+
+int lscomp_decompress_u16_async(lscomp_workspace *ws, const uint8_t *d_in, uint64_t cmp_len, uint32_t x,
+                                uint32_t y, uint32_t z, const uint32_t bins[4], float pooling,
+                                uint16_t *d_out, void *stream);
+
+/* Wait for the workspace's last launch on `stream` and return its status. */
+int lscomp_workspace_check(lscomp_workspace *ws, void *stream);
+
+/* Number of kernel launches this library has issued in this process (for
+   the benchmark's launch count). */
+uint64_t lscomp_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LSCOMP_H */

@@ -1,0 +1,88 @@
+// bitplane.h -- register-level bit-plane transposes shared by the encoder and
+// decoder kernels (and compiled on the host by the unit test of the format).
+//
+// Stream format of one 8x8 block (lsCOMP/src/cuLSZ_kernel.cu:1100-1276):
+//   plain block,  plane i (least significant first) = 8 bytes, byte r = row r,
+//                 bit (7-k) of that byte = bit i of the quantised value at col k;
+//   pooled block, plane i = 4 bytes, byte b = pooled values 8b..8b+7, the first
+//                 value in the most significant bit.
+// Here one thread holds the 8 quantised values of one row (or of one pooled
+// row pair) as four packed words w0..w3 (w0 = q0 | q1 << 16, ...).  The
+// functions below turn them into the 8 plane bytes for planes 0-7 (low value
+// bytes) or 8-15 (high value bytes), and back.
+#pragma once
+#include <stdint.h>
+
+#if defined(__CUDACC__)
+#define LSC_HD __host__ __device__ __forceinline__
+#else
+#define LSC_HD static inline
+#endif
+
+// Byte permute with the semantics of the PRMT instruction / __byte_perm:
+// result byte n = byte (sel >> 4n) & 7 of the 8-byte value {b:a}.
+LSC_HD uint32_t lsc_prmt(uint32_t a, uint32_t b, uint32_t sel)
+{
+#if defined(__CUDA_ARCH__)
+    return __byte_perm(a, b, sel);
+#else
+    uint64_t v = ((uint64_t)b << 32) | a;
+    uint32_t r = 0;
+    for (int n = 0; n < 4; n++) {
+        uint32_t s = (sel >> (4 * n)) & 7;
+        r |= (uint32_t)((v >> (8 * s)) & 0xff) << (8 * n);
+    }
+    return r;
+#endif
+}
+
+// 8x8 bit-matrix transpose of the 64-bit value {hi:lo}: bit (8a + b) moves to
+// bit (8b + a).  Three rounds of masked swaps (rows 1 apart, 2 apart, 4 apart);
+// the last round exchanges nibbles between the two 32-bit halves.  It is its
+// own inverse.
+LSC_HD void lsc_transpose8x8(uint32_t &lo, uint32_t &hi)
+{
+    uint32_t t;
+    t = (lo ^ (lo >> 7)) & 0x00AA00AAu; lo ^= t ^ (t << 7);
+    t = (hi ^ (hi >> 7)) & 0x00AA00AAu; hi ^= t ^ (t << 7);
+    t = (lo ^ (lo >> 14)) & 0x0000CCCCu; lo ^= t ^ (t << 14);
+    t = (hi ^ (hi >> 14)) & 0x0000CCCCu; hi ^= t ^ (t << 14);
+    t = (lo ^ (hi << 4)) & 0xF0F0F0F0u; lo ^= t; hi ^= t >> 4;
+}
+
+// Plane bytes of one row: w0..w3 hold q0..q7 (q_k in 16-bit half k&1 of
+// w[k>>1]).  high=0 gives planes 0-7, high=1 planes 8-15; on return p_lo holds
+// planes {0,1,2,3}(+8) in bytes 0..3 and p_hi planes {4,5,6,7}(+8).
+// The value bytes are laid out in reverse (q7 first) so that after the
+// transpose value k lands in bit 7-k of each plane byte.
+LSC_HD void lsc_row_planes(uint32_t w0, uint32_t w1, uint32_t w2, uint32_t w3, int high, uint32_t &p_lo,
+                           uint32_t &p_hi)
+{
+    uint32_t sel = high ? 0x5713u : 0x4602u;
+    uint32_t lo = lsc_prmt(w3, w2, sel); // q7 q6 q5 q4
+    uint32_t hi = lsc_prmt(w1, w0, sel); // q3 q2 q1 q0
+    lsc_transpose8x8(lo, hi);
+    p_lo = lo;
+    p_hi = hi;
+}
+
+// Inverse of lsc_row_planes for both halves at once: from the plane bytes of
+// planes 0-7 (l_lo, l_hi) and 8-15 (h_lo, h_hi) rebuild w0..w3.
+LSC_HD void lsc_row_values(uint32_t l_lo, uint32_t l_hi, uint32_t h_lo, uint32_t h_hi, uint32_t &w0,
+                           uint32_t &w1, uint32_t &w2, uint32_t &w3)
+{
+    lsc_transpose8x8(l_lo, l_hi); // value low bytes: l_lo = q7 q6 q5 q4, l_hi = q3 q2 q1 q0
+    lsc_transpose8x8(h_lo, h_hi); // value high bytes
+    w3 = lsc_prmt(l_lo, h_lo, 0x4051u);
+    w2 = lsc_prmt(l_lo, h_lo, 0x6273u);
+    w1 = lsc_prmt(l_hi, h_hi, 0x4051u);
+    w0 = lsc_prmt(l_hi, h_hi, 0x6273u);
+}
+
+// Second step of the 4x4 byte transpose across four threads (after the
+// exchange with the thread two rows away, see the kernels): selectors for
+// the even and the odd member of each pair.
+#define LSC_XP_A_LOW 0x5410u   // keep own bytes 0,1, take partner bytes 0,1
+#define LSC_XP_A_HIGH 0x7632u  // take partner bytes 2,3, keep own bytes 2,3 (partner first)
+#define LSC_XP_B_EVEN 0x6240u
+#define LSC_XP_B_ODD 0x3715u

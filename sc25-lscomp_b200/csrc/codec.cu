@@ -1,0 +1,384 @@
+// codec.cu -- host side of the uint16 codec: argument checks, tile geometry,
+// workspace (scan state + launch control block), kernel selection and the
+// C ABI declared in include/lscomp.h.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <atomic>
+#include <mutex>
+#include "lscomp.h"
+#include "codec_kernels.cuh"
+
+using namespace lsc;
+
+namespace {
+
+std::atomic<uint64_t> g_launches{0};
+
+constexpr uint32_t kEpochMax = (1u << 20) - 1;
+
+struct KernelShape {
+    int enc_ctas_per_sm = 0;
+    int dec_ctas_per_sm = 0;
+};
+
+}  // namespace
+
+struct lscomp_workspace {
+    int device = 0;
+    int sm_count = 0;
+    LaunchCtl *ctl = nullptr;          // device
+    LaunchCtl *h_ctl = nullptr;        // pinned host mirror for status reads
+    unsigned long long *state = nullptr;
+    uint64_t state_cap = 0;            // entries
+    uint32_t epoch = 0;
+    std::mutex mu;
+};
+
+namespace {
+
+int cuda_status(cudaError_t e)
+{
+    if (e == cudaSuccess) return LSCOMP_OK;
+    if (e == cudaErrorMemoryAllocation) return LSCOMP_ERR_NOMEM;
+    return LSCOMP_ERR_CUDA;
+}
+
+int dev_status(uint32_t e)
+{
+    switch (e) {
+    case DEV_OK: return LSCOMP_OK;
+    case DEV_ERR_TIMEOUT: return LSCOMP_ERR_TIMEOUT;
+    case DEV_ERR_CAPACITY: return LSCOMP_ERR_CAPACITY;
+    case DEV_ERR_CORRUPT: return LSCOMP_ERR_CORRUPT;
+    case DEV_ERR_RANGE: return LSCOMP_ERR_RANGE;
+    default: return LSCOMP_ERR_CUDA;
+    }
+}
+
+// smallest zero count k (0..64) with (float)k/64 > p, 65 if none
+// (lsCOMP/src/cuLSZ_kernel.cu:920-921; k/64 is exact in binary32)
+int pool_min_zeros(float p)
+{
+    for (int k = 0; k <= 64; k++) {
+        float sparsity = (float)k / 64.0f;
+        if (sparsity > p) return k;
+    }
+    return 65;
+}
+
+bool make_geom(uint32_t X, uint32_t Y, uint32_t Z, Geom &g)
+{
+    if (!X || !Y || !Z) return false;
+    g.X = X; g.Y = Y; g.Z = Z;
+    g.byb = (Y + 7) / 8;
+    g.bzb = (Z + 7) / 8;
+    g.nrows_b = (unsigned long long)X * g.byb;
+    g.nb = g.nrows_b * g.bzb;
+    g.R = (g.nb + 3) / 4 * 4;
+    g.N = (unsigned long long)X * Y * Z;
+    if (g.bzb <= (uint32_t)kTileBlocks) {
+        g.chunked = 0;
+        g.G = (uint32_t)kTileBlocks / g.bzb;
+        g.ntiles = (g.nrows_b + g.G - 1) / g.G;
+        g.nc = 1;
+        g.W = g.bzb;
+        g.inv_bzb = (65536u + g.bzb - 1) / g.bzb;
+    } else {
+        g.chunked = 1;
+        g.G = 1;
+        g.nc = (g.bzb + kTileBlocks - 1) / kTileBlocks;
+        g.W = (g.bzb + g.nc - 1) / g.nc;
+        g.ntiles = g.nrows_b * g.nc;
+        g.inv_bzb = 0;
+    }
+    return true;
+}
+
+bool make_codec(const uint32_t bins[4], float p, Codec &c, int &layout)
+{
+    if (!bins) return false;
+    for (int k = 0; k < 4; k++) {
+        if (bins[k] == 0) return false;
+        c.bins[k] = bins[k];
+        c.magic[k] = bins[k] == 1 ? 0u : (uint32_t)((0x100000000ull + bins[k] - 1) / bins[k]);
+        c.binc[k] = bins[k] > 65536u ? 65536u : bins[k];
+    }
+    c.pool_min = pool_min_zeros(p);
+    if (bins[0] == bins[1] && bins[1] == bins[2] && bins[2] == bins[3])
+        layout = BINS_EQUAL;
+    else if (bins[0] <= bins[1] && bins[1] <= bins[2] && bins[2] <= bins[3])
+        layout = BINS_MONO;
+    else
+        layout = BINS_GENERAL;
+    return true;
+}
+
+int vec_class(const void *p, uint32_t Z)
+{
+    uintptr_t a = reinterpret_cast<uintptr_t>(p);
+    if ((Z % 8u) == 0 && (a % 16u) == 0) return 16;
+    if ((Z % 2u) == 0 && (a % 4u) == 0) return 4;
+    return 2;
+}
+
+// Ensure the workspace holds `ntiles` scan slots and hand out a fresh epoch.
+int ws_prepare(lscomp_workspace *ws, uint64_t ntiles, cudaStream_t st)
+{
+    if (ntiles > ws->state_cap) {
+        uint64_t cap = ntiles + ntiles / 4 + 1024;
+        unsigned long long *p = nullptr;
+        cudaError_t e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return cuda_status(e);
+        if (ws->state) cudaFree(ws->state);
+        ws->state = nullptr;
+        ws->state_cap = 0;
+        e = cudaMalloc(&p, cap * sizeof(unsigned long long));
+        if (e != cudaSuccess) return cuda_status(e);
+        e = cudaMemsetAsync(p, 0, cap * sizeof(unsigned long long), st);
+        if (e != cudaSuccess) { cudaFree(p); return cuda_status(e); }
+        ws->state = p;
+        ws->state_cap = cap;
+        ws->epoch = 0;
+    }
+    if (ws->epoch >= kEpochMax) {
+        cudaError_t e = cudaMemsetAsync(ws->state, 0, ws->state_cap * sizeof(unsigned long long), st);
+        if (e != cudaSuccess) return cuda_status(e);
+        ws->epoch = 0;
+    }
+    ws->epoch++;
+    cudaError_t e = cudaMemsetAsync(ws->ctl, 0, sizeof(LaunchCtl), st);
+    return cuda_status(e);
+}
+
+template <typename K>
+int ctas_per_sm(K kernel, size_t smem)
+{
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, kThreads, smem) != cudaSuccess) return 1;
+    return n > 0 ? n : 1;
+}
+
+template <int VEC, int BINS, bool POOL>
+int launch_enc_t(const EncArgs &a, int sm_count, cudaStream_t st)
+{
+    auto k = enc_kernel<VEC, BINS, POOL>;
+    const size_t smem = sizeof(EncSmem);
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    static int per_sm = 0;
+    if (!per_sm) per_sm = ctas_per_sm(k, smem);
+    unsigned long long grid = (unsigned long long)sm_count * per_sm;
+    if (grid > a.g.ntiles) grid = a.g.ntiles;
+    k<<<(unsigned)grid, kThreads, smem, st>>>(a);
+    g_launches.fetch_add(1);
+    return cuda_status(cudaGetLastError());
+}
+
+template <int VEC>
+int launch_enc_v(const EncArgs &a, int layout, bool pool, int sm, cudaStream_t st)
+{
+    if (layout == BINS_EQUAL)
+        return pool ? launch_enc_t<VEC, BINS_EQUAL, true>(a, sm, st) : launch_enc_t<VEC, BINS_EQUAL, false>(a, sm, st);
+    if (layout == BINS_MONO)
+        return pool ? launch_enc_t<VEC, BINS_MONO, true>(a, sm, st) : launch_enc_t<VEC, BINS_MONO, false>(a, sm, st);
+    return pool ? launch_enc_t<VEC, BINS_GENERAL, true>(a, sm, st) : launch_enc_t<VEC, BINS_GENERAL, false>(a, sm, st);
+}
+
+template <int VEC>
+int launch_dec_t(const DecArgs &a, int sm_count, cudaStream_t st)
+{
+    auto k = dec_kernel<VEC>;
+    static int per_sm = 0;
+    if (!per_sm) per_sm = ctas_per_sm(k, 0);
+    unsigned long long grid = (unsigned long long)sm_count * per_sm;
+    if (grid > a.g.ntiles) grid = a.g.ntiles;
+    k<<<(unsigned)grid, kThreads, 0, st>>>(a);
+    g_launches.fetch_add(1);
+    return cuda_status(cudaGetLastError());
+}
+
+int read_ctl(lscomp_workspace *ws, cudaStream_t st)
+{
+    cudaError_t e = cudaMemcpyAsync(ws->h_ctl, ws->ctl, sizeof(LaunchCtl), cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) return cuda_status(e);
+    e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_status(e);
+    return dev_status(ws->h_ctl->error);
+}
+
+}  // namespace
+
+extern "C" {
+
+int lscomp_version(void) { return 100; }
+
+const char *lscomp_status_string(int s)
+{
+    switch (s) {
+    case LSCOMP_OK: return "ok";
+    case LSCOMP_ERR_ARG: return "invalid argument";
+    case LSCOMP_ERR_CAPACITY: return "buffer too small for the stream";
+    case LSCOMP_ERR_CUDA: return "CUDA runtime error";
+    case LSCOMP_ERR_TIMEOUT: return "bounded wait in kernel timed out";
+    case LSCOMP_ERR_CORRUPT: return "stream inconsistent with the geometry";
+    case LSCOMP_ERR_RANGE: return "value range not representable";
+    case LSCOMP_ERR_NOMEM: return "out of memory";
+    default: return "unknown status";
+    }
+}
+
+uint64_t lscomp_block_count(uint32_t x, uint32_t y, uint32_t z)
+{
+    return (uint64_t)x * ((y + 7) / 8) * ((z + 7) / 8);
+}
+
+uint64_t lscomp_max_stream_bytes_u16(uint32_t x, uint32_t y, uint32_t z)
+{
+    uint64_t nb = lscomp_block_count(x, y, z);
+    return (nb + 3) / 4 * 4 + 128ull * nb;
+}
+
+uint64_t lscomp_launch_count(void) { return g_launches.load(); }
+
+int lscomp_workspace_create(lscomp_workspace **out, int device)
+{
+    if (!out) return LSCOMP_ERR_ARG;
+    *out = nullptr;
+    int dev = device;
+    if (dev < 0 && cudaGetDevice(&dev) != cudaSuccess) return LSCOMP_ERR_CUDA;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (cudaSetDevice(dev) != cudaSuccess) return LSCOMP_ERR_CUDA;
+    lscomp_workspace *ws = new (std::nothrow) lscomp_workspace();
+    if (!ws) return LSCOMP_ERR_NOMEM;
+    ws->device = dev;
+    int st = LSCOMP_OK;
+    if (cudaDeviceGetAttribute(&ws->sm_count, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) st = LSCOMP_ERR_CUDA;
+    if (!st) st = cuda_status(cudaMalloc(&ws->ctl, sizeof(LaunchCtl)));
+    if (!st) st = cuda_status(cudaMemset(ws->ctl, 0, sizeof(LaunchCtl)));
+    if (!st) st = cuda_status(cudaMallocHost(&ws->h_ctl, sizeof(LaunchCtl)));
+    cudaSetDevice(prev);
+    if (st) {
+        lscomp_workspace_destroy(ws);
+        return st;
+    }
+    *out = ws;
+    return LSCOMP_OK;
+}
+
+int lscomp_workspace_destroy(lscomp_workspace *ws)
+{
+    if (!ws) return LSCOMP_OK;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(ws->device);
+    if (ws->state) cudaFree(ws->state);
+    if (ws->ctl) cudaFree(ws->ctl);
+    if (ws->h_ctl) cudaFreeHost(ws->h_ctl);
+    cudaSetDevice(prev);
+    delete ws;
+    return LSCOMP_OK;
+}
+
+int lscomp_workspace_check(lscomp_workspace *ws, void *stream)
+{
+    if (!ws) return LSCOMP_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ws->mu);
+    return read_ctl(ws, (cudaStream_t)stream);
+}
+
+int lscomp_compress_u16_async(lscomp_workspace *ws, const uint16_t *d_in, uint32_t x, uint32_t y, uint32_t z,
+                              const uint32_t bins[4], float pooling, uint8_t *d_out, uint64_t cap,
+                              uint64_t *d_sizes, void *stream)
+{
+    if (!ws || !d_in || !d_out) return LSCOMP_ERR_ARG;
+    if (reinterpret_cast<uintptr_t>(d_in) & 1u) return LSCOMP_ERR_ARG;
+    EncArgs a;
+    int layout = 0;
+    if (!make_geom(x, y, z, a.g) || !make_codec(bins, pooling, a.c, layout)) return LSCOMP_ERR_ARG;
+    if (cap < a.g.R) return LSCOMP_ERR_CAPACITY;
+    cudaStream_t st = (cudaStream_t)stream;
+    std::lock_guard<std::mutex> lk(ws->mu);
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (prev != ws->device) cudaSetDevice(ws->device);
+    int s = ws_prepare(ws, a.g.ntiles, st);
+    if (!s) {
+        a.in = d_in;
+        a.out = d_out;
+        a.cap = cap;
+        a.ctl = ws->ctl;
+        a.state = ws->state;
+        a.epoch = ws->epoch;
+        a.sizes_out = reinterpret_cast<unsigned long long *>(d_sizes);
+        const bool pool = a.c.pool_min <= 64;
+        switch (vec_class(d_in, z)) {
+        case 16: s = launch_enc_v<16>(a, layout, pool, ws->sm_count, st); break;
+        case 4: s = launch_enc_v<4>(a, layout, pool, ws->sm_count, st); break;
+        default: s = launch_enc_v<2>(a, layout, pool, ws->sm_count, st); break;
+        }
+    }
+    if (prev != ws->device) cudaSetDevice(prev);
+    return s;
+}
+
+int lscomp_compress_u16(lscomp_workspace *ws, const uint16_t *d_in, uint32_t x, uint32_t y, uint32_t z,
+                        const uint32_t bins[4], float pooling, uint8_t *d_out, uint64_t cap,
+                        uint64_t *stream_len, uint64_t *ref_size, void *stream)
+{
+    int s = lscomp_compress_u16_async(ws, d_in, x, y, z, bins, pooling, d_out, cap, nullptr, stream);
+    if (s) return s;
+    std::lock_guard<std::mutex> lk(ws->mu);
+    s = read_ctl(ws, (cudaStream_t)stream);
+    if (s) return s;
+    uint64_t nb = lscomp_block_count(x, y, z);
+    if (stream_len) *stream_len = ws->h_ctl->stream_len;
+    if (ref_size) *ref_size = ws->h_ctl->total + nb;
+    return LSCOMP_OK;
+}
+
+int lscomp_decompress_u16_async(lscomp_workspace *ws, const uint8_t *d_in, uint64_t cmp_len, uint32_t x,
+                                uint32_t y, uint32_t z, const uint32_t bins[4], float pooling, uint16_t *d_out,
+                                void *stream)
+{
+    if (!ws || !d_in || !d_out) return LSCOMP_ERR_ARG;
+    if (reinterpret_cast<uintptr_t>(d_out) & 1u) return LSCOMP_ERR_ARG;
+    DecArgs a;
+    int layout = 0;
+    if (!make_geom(x, y, z, a.g) || !make_codec(bins, pooling, a.c, layout)) return LSCOMP_ERR_ARG;
+    if (cmp_len < a.g.nb) return LSCOMP_ERR_CAPACITY;
+    cudaStream_t st = (cudaStream_t)stream;
+    std::lock_guard<std::mutex> lk(ws->mu);
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (prev != ws->device) cudaSetDevice(ws->device);
+    int s = ws_prepare(ws, a.g.ntiles, st);
+    if (!s) {
+        a.in = d_in;
+        a.out = d_out;
+        a.cap = cmp_len;
+        a.ctl = ws->ctl;
+        a.state = ws->state;
+        a.epoch = ws->epoch;
+        switch (vec_class(d_out, z)) {
+        case 16: s = launch_dec_t<16>(a, ws->sm_count, st); break;
+        case 4: s = launch_dec_t<4>(a, ws->sm_count, st); break;
+        default: s = launch_dec_t<2>(a, ws->sm_count, st); break;
+        }
+    }
+    if (prev != ws->device) cudaSetDevice(prev);
+    return s;
+}
+
+int lscomp_decompress_u16(lscomp_workspace *ws, const uint8_t *d_in, uint64_t cmp_len, uint32_t x, uint32_t y,
+                          uint32_t z, const uint32_t bins[4], float pooling, uint16_t *d_out, void *stream)
+{
+    int s = lscomp_decompress_u16_async(ws, d_in, cmp_len, x, y, z, bins, pooling, d_out, stream);
+    if (s) return s;
+    std::lock_guard<std::mutex> lk(ws->mu);
+    return read_ctl(ws, (cudaStream_t)stream);
+}
+
+}  // extern "C"

@@ -1,0 +1,272 @@
+"""Python host interface of the B200 lsCOMP codec (uint16 detector stacks).
+
+Mirrors the reference's host API (lsCOMP/include/cuLSZ_entry.h:8-11):
+
+    compress(data, dims, bins, pooling)   ~ cuLSZ_compression_uint16_bsize64
+    decompress(stream, dims, bins, pooling) ~ cuLSZ_decompression_uint16_bsize64
+
+with the same argument meaning (dims = (x, y, z), z fastest; four
+quantisation bins; the -p pooling threshold) and the same stream format.
+Device buffers are torch tensors on a CUDA device (uint16 data is carried in
+int16 tensors, bit for bit).  Every call goes through the C ABI of
+liblscomp.so (include/lscomp.h); there is no other implementation, so a
+missing or unloadable library raises instead of falling back.
+
+The synthetic stack generators used by the tests and the benchmark live in
+liblscomp_synth.so and are exposed as synth_small / synth_cssi / synth_xpcs.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Sequence, Tuple
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "liblscomp.so")
+SYNTH_PATH = os.path.join(_HERE, "liblscomp_synth.so")
+
+STATUS = {
+    0: "ok",
+    1: "invalid argument",
+    2: "buffer too small for the stream",
+    3: "CUDA runtime error",
+    4: "bounded wait in kernel timed out",
+    5: "stream inconsistent with the geometry",
+    6: "value range not representable",
+    7: "out of memory",
+}
+
+
+class LscompError(RuntimeError):
+    def __init__(self, status: int, what: str):
+        self.status = status
+        super().__init__(f"{what}: {STATUS.get(status, 'unknown')} (status {status})")
+
+
+_lib = None
+_synth_lib = None
+
+
+def _u32(x):
+    return ctypes.c_uint32(int(x))
+
+
+def load_library() -> ctypes.CDLL:
+    """Load liblscomp.so (built by `make -C sc25-lscomp_b200`)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"liblscomp.so not built: {LIB_PATH} (run __graft_entry__.build())")
+    lib = ctypes.CDLL(LIB_PATH)
+    vp, u32, u64, f32 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_float
+    pu64 = ctypes.POINTER(ctypes.c_uint64)
+    bins_t = ctypes.POINTER(ctypes.c_uint32)
+    lib.lscomp_version.restype = ctypes.c_int
+    lib.lscomp_status_string.restype = ctypes.c_char_p
+    lib.lscomp_status_string.argtypes = [ctypes.c_int]
+    lib.lscomp_block_count.restype = u64
+    lib.lscomp_block_count.argtypes = [u32, u32, u32]
+    lib.lscomp_max_stream_bytes_u16.restype = u64
+    lib.lscomp_max_stream_bytes_u16.argtypes = [u32, u32, u32]
+    lib.lscomp_launch_count.restype = u64
+    lib.lscomp_workspace_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int]
+    lib.lscomp_workspace_destroy.argtypes = [vp]
+    lib.lscomp_workspace_check.argtypes = [vp, vp]
+    lib.lscomp_compress_u16.argtypes = [vp, vp, u32, u32, u32, bins_t, f32, vp, u64, pu64, pu64, vp]
+    lib.lscomp_compress_u16_async.argtypes = [vp, vp, u32, u32, u32, bins_t, f32, vp, u64, vp, vp]
+    lib.lscomp_decompress_u16.argtypes = [vp, vp, u64, u32, u32, u32, bins_t, f32, vp, vp]
+    lib.lscomp_decompress_u16_async.argtypes = [vp, vp, u64, u32, u32, u32, bins_t, f32, vp, vp]
+    _lib = lib
+    return lib
+
+
+def _check(st: int, what: str):
+    if st != 0:
+        raise LscompError(st, what)
+
+
+def _bins(bins: Sequence[int]):
+    if len(bins) != 4:
+        raise ValueError("bins must have four entries")
+    arr = (ctypes.c_uint32 * 4)(*[int(b) for b in bins])
+    return arr
+
+
+def block_count(dims: Sequence[int]) -> int:
+    x, y, z = dims
+    return x * ((y + 7) // 8) * ((z + 7) // 8)
+
+
+def max_stream_bytes(dims: Sequence[int]) -> int:
+    nb = block_count(dims)
+    return (nb + 3) // 4 * 4 + 128 * nb
+
+
+def launch_count() -> int:
+    return int(load_library().lscomp_launch_count())
+
+
+class Workspace:
+    """Scan state for a sequence of ordered calls on one device."""
+
+    def __init__(self, device: int = -1):
+        lib = load_library()
+        self._ws = ctypes.c_void_p()
+        _check(lib.lscomp_workspace_create(ctypes.byref(self._ws), int(device)), "lscomp_workspace_create")
+
+    @property
+    def handle(self):
+        return self._ws
+
+    def close(self):
+        if self._ws:
+            load_library().lscomp_workspace_destroy(self._ws)
+            self._ws = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def check(self, stream: int = 0):
+        _check(load_library().lscomp_workspace_check(self._ws, ctypes.c_void_p(stream)), "lscomp_workspace_check")
+
+
+def _stream_handle(stream) -> int:
+    if stream is None:
+        import torch
+
+        return torch.cuda.current_stream().cuda_stream
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+def compress_into(ws: Workspace, d_in, dims, bins, pooling: float, d_out, stream=None) -> Tuple[int, int]:
+    """Compress device tensor d_in (X*Y*Z uint16 in int16) into d_out (uint8).
+
+    Returns (stream_len, ref_size): the stream's length in bytes and the size
+    the reference's host API reports (payload + nb)."""
+    lib = load_library()
+    x, y, z = (int(v) for v in dims)
+    sl, rs = ctypes.c_uint64(0), ctypes.c_uint64(0)
+    st = lib.lscomp_compress_u16(
+        ws.handle, ctypes.c_void_p(d_in.data_ptr()), x, y, z, _bins(bins), ctypes.c_float(pooling),
+        ctypes.c_void_p(d_out.data_ptr()), ctypes.c_uint64(d_out.numel() * d_out.element_size()),
+        ctypes.byref(sl), ctypes.byref(rs), ctypes.c_void_p(_stream_handle(stream)))
+    _check(st, "lscomp_compress_u16")
+    return int(sl.value), int(rs.value)
+
+
+def compress_async(ws: Workspace, d_in, dims, bins, pooling: float, d_out, d_sizes=None, stream=None):
+    """Enqueue a compression without host synchronisation; d_sizes (2 x uint64
+    in an int64 tensor) receives {stream_len, payload bytes}."""
+    lib = load_library()
+    x, y, z = (int(v) for v in dims)
+    st = lib.lscomp_compress_u16_async(
+        ws.handle, ctypes.c_void_p(d_in.data_ptr()), x, y, z, _bins(bins), ctypes.c_float(pooling),
+        ctypes.c_void_p(d_out.data_ptr()), ctypes.c_uint64(d_out.numel() * d_out.element_size()),
+        ctypes.c_void_p(d_sizes.data_ptr() if d_sizes is not None else 0),
+        ctypes.c_void_p(_stream_handle(stream)))
+    _check(st, "lscomp_compress_u16_async")
+
+
+def decompress_into(ws: Workspace, d_cmp, cmp_len: int, dims, bins, pooling: float, d_out, stream=None):
+    """Decompress the stream in device tensor d_cmp (cmp_len readable bytes)
+    into d_out (X*Y*Z uint16 in int16)."""
+    lib = load_library()
+    x, y, z = (int(v) for v in dims)
+    st = lib.lscomp_decompress_u16(
+        ws.handle, ctypes.c_void_p(d_cmp.data_ptr()), ctypes.c_uint64(int(cmp_len)), x, y, z, _bins(bins),
+        ctypes.c_float(pooling), ctypes.c_void_p(d_out.data_ptr()), ctypes.c_void_p(_stream_handle(stream)))
+    _check(st, "lscomp_decompress_u16")
+
+
+def decompress_async(ws: Workspace, d_cmp, cmp_len: int, dims, bins, pooling: float, d_out, stream=None):
+    lib = load_library()
+    x, y, z = (int(v) for v in dims)
+    st = lib.lscomp_decompress_u16_async(
+        ws.handle, ctypes.c_void_p(d_cmp.data_ptr()), ctypes.c_uint64(int(cmp_len)), x, y, z, _bins(bins),
+        ctypes.c_float(pooling), ctypes.c_void_p(d_out.data_ptr()), ctypes.c_void_p(_stream_handle(stream)))
+    _check(st, "lscomp_decompress_u16_async")
+
+
+_default_ws = {}
+
+
+def _ws_for(device: int) -> Workspace:
+    if device not in _default_ws:
+        _default_ws[device] = Workspace(device)
+    return _default_ws[device]
+
+
+def compress(data, dims, bins, pooling: float, out=None, stream=None):
+    """Reference-style call: returns (stream tensor, cmp_size) where cmp_size
+    is what cuLSZ_compression_uint16_bsize64 reports; the stream tensor is
+    trimmed to the true stream length."""
+    import torch
+
+    dev = data.device.index if data.device.index is not None else torch.cuda.current_device()
+    if out is None:
+        out = torch.empty(max_stream_bytes(dims), dtype=torch.uint8, device=data.device)
+    sl, rs = compress_into(_ws_for(dev), data, dims, bins, pooling, out, stream)
+    return out[:sl], rs
+
+
+def decompress(stream_t, dims, bins, pooling: float, out=None, stream=None):
+    import torch
+
+    dev = stream_t.device.index if stream_t.device.index is not None else torch.cuda.current_device()
+    if out is None:
+        n = int(dims[0]) * int(dims[1]) * int(dims[2])
+        out = torch.empty(n, dtype=torch.int16, device=stream_t.device)
+    decompress_into(_ws_for(dev), stream_t, stream_t.numel(), dims, bins, pooling, out, stream)
+    return out
+
+
+# --------------------------------------------------------------- synthetic data
+def _load_synth():
+    global _synth_lib
+    if _synth_lib is None:
+        if not os.path.exists(SYNTH_PATH):
+            raise ImportError(f"liblscomp_synth.so not built: {SYNTH_PATH}")
+        s = ctypes.CDLL(SYNTH_PATH)
+        for name in ("lsc_synth_small", "lsc_synth_cssi", "lsc_synth_xpcs"):
+            f = getattr(s, name)
+            f.restype = ctypes.c_int
+            f.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                          ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int]
+        _synth_lib = s
+    return _synth_lib
+
+
+def _synth(kind: str, dims, seed: int, frames: Optional[Tuple[int, int]] = None, out=None, threads: int = 0):
+    x, y, z = (int(v) for v in dims)
+    x0, nx = frames if frames is not None else (0, x)
+    if out is None:
+        out = np.empty(nx * y * z, dtype=np.uint16)
+    assert out.dtype == np.uint16 and out.size >= nx * y * z and out.flags["C_CONTIGUOUS"]
+    f = getattr(_load_synth(), f"lsc_synth_{kind}")
+    st = f(out.ctypes.data, x, y, z, x0, nx, ctypes.c_uint64(seed), threads)
+    if st != 0:
+        raise RuntimeError(f"lsc_synth_{kind} failed ({st})")
+    return out
+
+
+def synth_small(dims, seed: int = 1, frames=None, out=None, threads: int = 0):
+    """Poisson(0.1) background, 20 Gaussian spots per frame, 0.1% hot pixels."""
+    return _synth("small", dims, seed, frames, out, threads)
+
+
+def synth_cssi(dims, seed: int = 2, frames=None, out=None, threads: int = 0):
+    """Radial Poisson background 50 -> 0.5, 3-8 diffraction rings, beamstop."""
+    return _synth("cssi", dims, seed, frames, out, threads)
+
+
+def synth_xpcs(dims, seed: int = 3, frames=None, out=None, threads: int = 0):
+    """Sparse AR(1) speckle (mean 0.02, rho 0.9), beamstop disk r = 60 px."""
+    return _synth("xpcs", dims, seed, frames, out, threads)
