@@ -17,6 +17,10 @@
  *   lscomp_decompress_u16 / _async   cuLSZ_decompression_uint16_bsize64
  *                                    (lsCOMP/include/cuLSZ_entry.h:11,
  *                                     lsCOMP/src/cuLSZ_entry.cu:133-166)
+ *   lscomp_compress_u32 / _async     cuLSZ_compression_uint32_bsize64
+ *                                    (lsCOMP/include/cuLSZ_entry.h:8, cuLSZ_entry.cu:18-56)
+ *   lscomp_decompress_u32 / _async   cuLSZ_decompression_uint32_bsize64
+ *                                    (lsCOMP/include/cuLSZ_entry.h:9, cuLSZ_entry.cu:58-91)
  *   lscomp_workspace_*               the per-call cudaMalloc/cudaMemset/cudaFree
  *                                    of the scan scratch (cuLSZ_entry.cu:105-114,
  *                                    128-130), made reusable
@@ -85,6 +89,25 @@ int lscomp_decompress_u16(lscomp_workspace *ws, const uint8_t *d_in, uint64_t cm
 int lscomp_decompress_u16_async(lscomp_workspace *ws, const uint8_t *d_in, uint64_t cmp_len, uint32_t x,
                                 uint32_t y, uint32_t z, const uint32_t bins[4], float pooling,
                                 uint16_t *d_out, void *stream);
+
+/* uint32 twins (lsCOMP/include/cuLSZ_entry.h:8-9, lsCOMP/src/cuLSZ_entry.cu:18-91).
+   Same stream format; a block whose quantised maximum needs 32 bit planes
+   (a quotient >= 2^31) cannot be represented in the 5-bit rate field and
+   fails with LSCOMP_ERR_RANGE.  Offsets are 64-bit (the reference's are
+   32-bit, so the two agree on streams below 4 GiB). */
+uint64_t lscomp_max_stream_bytes_u32(uint32_t x, uint32_t y, uint32_t z);
+int lscomp_compress_u32(lscomp_workspace *ws, const uint32_t *d_in, uint32_t x, uint32_t y, uint32_t z,
+                        const uint32_t bins[4], float pooling, uint8_t *d_out, uint64_t cap,
+                        uint64_t *stream_len, uint64_t *ref_size, void *stream);
+int lscomp_compress_u32_async(lscomp_workspace *ws, const uint32_t *d_in, uint32_t x, uint32_t y,
+                              uint32_t z, const uint32_t bins[4], float pooling, uint8_t *d_out,
+                              uint64_t cap, uint64_t *d_sizes, void *stream);
+int lscomp_decompress_u32(lscomp_workspace *ws, const uint8_t *d_in, uint64_t cmp_len, uint32_t x,
+                          uint32_t y, uint32_t z, const uint32_t bins[4], float pooling, uint32_t *d_out,
+                          void *stream);
+int lscomp_decompress_u32_async(lscomp_workspace *ws, const uint8_t *d_in, uint64_t cmp_len, uint32_t x,
+                                uint32_t y, uint32_t z, const uint32_t bins[4], float pooling,
+                                uint32_t *d_out, void *stream);
 
 /* Wait for the workspace's last launch on `stream` and return its status. */
 int lscomp_workspace_check(lscomp_workspace *ws, void *stream);

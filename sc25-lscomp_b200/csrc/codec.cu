@@ -19,11 +19,6 @@ std::atomic<uint64_t> g_launches{0};
 
 constexpr uint32_t kEpochMax = (1u << 20) - 1;
 
-struct KernelShape {
-    int enc_ctas_per_sm = 0;
-    int dec_ctas_per_sm = 0;
-};
-
 }  // namespace
 
 struct lscomp_workspace {
@@ -31,8 +26,8 @@ struct lscomp_workspace {
     int sm_count = 0;
     LaunchCtl *ctl = nullptr;          // device
     LaunchCtl *h_ctl = nullptr;        // pinned host mirror for status reads
-    unsigned long long *state = nullptr;
-    uint64_t state_cap = 0;            // entries
+    unsigned long long *state = nullptr;   // look-back words, then per-tile offsets
+    uint64_t state_cap = 0;            // entries of each of the two arrays
     uint32_t epoch = 0;
     std::mutex mu;
 };
@@ -69,7 +64,7 @@ int pool_min_zeros(float p)
     return 65;
 }
 
-bool make_geom(uint32_t X, uint32_t Y, uint32_t Z, Geom &g)
+bool make_geom(uint32_t X, uint32_t Y, uint32_t Z, uint32_t tile_blocks, Geom &g)
 {
     if (!X || !Y || !Z) return false;
     g.X = X; g.Y = Y; g.Z = Z;
@@ -79,9 +74,9 @@ bool make_geom(uint32_t X, uint32_t Y, uint32_t Z, Geom &g)
     g.nb = g.nrows_b * g.bzb;
     g.R = (g.nb + 3) / 4 * 4;
     g.N = (unsigned long long)X * Y * Z;
-    if (g.bzb <= (uint32_t)kTileBlocks) {
+    if (g.bzb <= tile_blocks) {
         g.chunked = 0;
-        g.G = (uint32_t)kTileBlocks / g.bzb;
+        g.G = tile_blocks / g.bzb;
         g.ntiles = (g.nrows_b + g.G - 1) / g.G;
         g.nc = 1;
         g.W = g.bzb;
@@ -89,7 +84,7 @@ bool make_geom(uint32_t X, uint32_t Y, uint32_t Z, Geom &g)
     } else {
         g.chunked = 1;
         g.G = 1;
-        g.nc = (g.bzb + kTileBlocks - 1) / kTileBlocks;
+        g.nc = (g.bzb + tile_blocks - 1) / tile_blocks;
         g.W = (g.bzb + g.nc - 1) / g.nc;
         g.ntiles = g.nrows_b * g.nc;
         g.inv_bzb = 0;
@@ -97,14 +92,23 @@ bool make_geom(uint32_t X, uint32_t Y, uint32_t Z, Geom &g)
     return true;
 }
 
-bool make_codec(const uint32_t bins[4], float p, Codec &c, int &layout)
+// ceil(2^64 / b) for b >= 2: with 2^64 - 1 = q b + r (0 <= r < b), 2^64 / b
+// = q + (r + 1) / b and 0 < r + 1 <= b, so the ceiling is always q + 1
+unsigned long long magic64(uint32_t b)
+{
+    if (b < 2) return 0;
+    return ~0ull / b + 1;
+}
+
+bool make_codec(const uint32_t bins[4], float p, bool wide, Codec &c, int &layout)
 {
     if (!bins) return false;
     for (int k = 0; k < 4; k++) {
         if (bins[k] == 0) return false;
         c.bins[k] = bins[k];
         c.magic[k] = bins[k] == 1 ? 0u : (uint32_t)((0x100000000ull + bins[k] - 1) / bins[k]);
-        c.binc[k] = bins[k] > 65536u ? 65536u : bins[k];
+        c.magic64[k] = magic64(bins[k]);
+        c.binc[k] = (!wide && bins[k] > 65536u) ? 65536u : bins[k];
     }
     c.pool_min = pool_min_zeros(p);
     if (bins[0] == bins[1] && bins[1] == bins[2] && bins[2] == bins[3])
@@ -116,12 +120,17 @@ bool make_codec(const uint32_t bins[4], float p, Codec &c, int &layout)
     return true;
 }
 
-int vec_class(const void *p, uint32_t Z)
+// widest access every row segment of the stack allows (bytes)
+int vec_class(const void *p, uint32_t Z, size_t es)
 {
     uintptr_t a = reinterpret_cast<uintptr_t>(p);
-    if ((Z % 8u) == 0 && (a % 16u) == 0) return 16;
-    if ((Z % 2u) == 0 && (a % 4u) == 0) return 4;
-    return 2;
+    if (es == 2) {
+        if ((Z % 8u) == 0 && (a % 16u) == 0) return 16;
+        if ((Z % 2u) == 0 && (a % 4u) == 0) return 4;
+        return 2;
+    }
+    if ((Z % 4u) == 0 && (a % 16u) == 0) return 16;
+    return 4;
 }
 
 // Ensure the workspace holds `ntiles` scan slots and hand out a fresh epoch.
@@ -135,9 +144,9 @@ int ws_prepare(lscomp_workspace *ws, uint64_t ntiles, cudaStream_t st)
         if (ws->state) cudaFree(ws->state);
         ws->state = nullptr;
         ws->state_cap = 0;
-        e = cudaMalloc(&p, cap * sizeof(unsigned long long));
+        e = cudaMalloc(&p, 2 * cap * sizeof(unsigned long long));
         if (e != cudaSuccess) return cuda_status(e);
-        e = cudaMemsetAsync(p, 0, cap * sizeof(unsigned long long), st);
+        e = cudaMemsetAsync(p, 0, 2 * cap * sizeof(unsigned long long), st);
         if (e != cudaSuccess) { cudaFree(p); return cuda_status(e); }
         ws->state = p;
         ws->state_cap = cap;
@@ -161,40 +170,47 @@ int ctas_per_sm(K kernel, size_t smem)
     return n > 0 ? n : 1;
 }
 
-template <int VEC, int BINS, bool POOL>
-int launch_enc_t(const EncArgs &a, int sm_count, cudaStream_t st)
+template <typename T, int VEC, int BINS, bool POOL>
+int launch_enc_t(const EncArgs<T> &a, int sm_count, cudaStream_t st)
 {
-    auto k = enc_kernel<VEC, BINS, POOL>;
+    auto k = enc_kernel<T, VEC, BINS, POOL>;
     const size_t smem = sizeof(EncSmem);
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    static int per_sm = 0;
-    if (!per_sm) per_sm = ctas_per_sm(k, smem);
-    unsigned long long grid = (unsigned long long)sm_count * per_sm;
+    // persistent: one CTA per SM (the CTA holds ~200 KB of rings)
+    unsigned long long grid = (unsigned long long)sm_count;
     if (grid > a.g.ntiles) grid = a.g.ntiles;
-    k<<<(unsigned)grid, kThreads, smem, st>>>(a);
+    k<<<(unsigned)grid, kEncThreads, smem, st>>>(a);
     g_launches.fetch_add(1);
     return cuda_status(cudaGetLastError());
 }
 
-template <int VEC>
-int launch_enc_v(const EncArgs &a, int layout, bool pool, int sm, cudaStream_t st)
+template <typename T, int VEC>
+int launch_enc_v(const EncArgs<T> &a, int layout, bool pool, int sm, cudaStream_t st)
 {
     if (layout == BINS_EQUAL)
-        return pool ? launch_enc_t<VEC, BINS_EQUAL, true>(a, sm, st) : launch_enc_t<VEC, BINS_EQUAL, false>(a, sm, st);
+        return pool ? launch_enc_t<T, VEC, BINS_EQUAL, true>(a, sm, st)
+                    : launch_enc_t<T, VEC, BINS_EQUAL, false>(a, sm, st);
     if (layout == BINS_MONO)
-        return pool ? launch_enc_t<VEC, BINS_MONO, true>(a, sm, st) : launch_enc_t<VEC, BINS_MONO, false>(a, sm, st);
-    return pool ? launch_enc_t<VEC, BINS_GENERAL, true>(a, sm, st) : launch_enc_t<VEC, BINS_GENERAL, false>(a, sm, st);
+        return pool ? launch_enc_t<T, VEC, BINS_MONO, true>(a, sm, st)
+                    : launch_enc_t<T, VEC, BINS_MONO, false>(a, sm, st);
+    return pool ? launch_enc_t<T, VEC, BINS_GENERAL, true>(a, sm, st)
+                : launch_enc_t<T, VEC, BINS_GENERAL, false>(a, sm, st);
 }
 
-template <int VEC>
-int launch_dec_t(const DecArgs &a, int sm_count, cudaStream_t st)
+template <typename T, int VEC>
+int launch_dec_t(const DecArgs<T> &a, int sm_count, cudaStream_t st)
 {
-    auto k = dec_kernel<VEC>;
-    static int per_sm = 0;
-    if (!per_sm) per_sm = ctas_per_sm(k, 0);
-    unsigned long long grid = (unsigned long long)sm_count * per_sm;
-    if (grid > a.g.ntiles) grid = a.g.ntiles;
-    k<<<(unsigned)grid, kThreads, 0, st>>>(a);
+    // 1) per-tile stream offsets from the header bytes
+    const unsigned long long nseg = (a.g.ntiles + kSegTiles - 1) / kSegTiles;
+    unsigned long long grid = (unsigned long long)sm_count * 4;
+    if (grid > nseg) grid = nseg;
+    dec_offsets_kernel<T><<<(unsigned)grid, kThreads, 0, st>>>(a);
+    g_launches.fetch_add(1);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_status(e);
+    // 2) every tile independently
+    if (a.g.ntiles > 0x7fffffffull) return LSCOMP_ERR_ARG;
+    dec_kernel<T, VEC><<<(unsigned)a.g.ntiles, kThreads, 0, st>>>(a);
     g_launches.fetch_add(1);
     return cuda_status(cudaGetLastError());
 }
@@ -208,7 +224,105 @@ int read_ctl(lscomp_workspace *ws, cudaStream_t st)
     return dev_status(ws->h_ctl->error);
 }
 
+template <typename T>
+int compress_async_t(lscomp_workspace *ws, const T *d_in, uint32_t x, uint32_t y, uint32_t z, const uint32_t bins[4],
+                     float pooling, uint8_t *d_out, uint64_t cap, uint64_t *d_sizes, void *stream)
+{
+    if (!ws || !d_in || !d_out) return LSCOMP_ERR_ARG;
+    // the stream is written in 4-byte words
+    if (reinterpret_cast<uintptr_t>(d_in) % sizeof(T) || reinterpret_cast<uintptr_t>(d_out) % 4u) return LSCOMP_ERR_ARG;
+    EncArgs<T> a;
+    int layout = 0;
+    if (!make_geom(x, y, z, Elem<T>::kTileBlocks, a.g) || !make_codec(bins, pooling, sizeof(T) == 4, a.c, layout))
+        return LSCOMP_ERR_ARG;
+    if (cap < a.g.R) return LSCOMP_ERR_CAPACITY;
+    cudaStream_t st = (cudaStream_t)stream;
+    std::lock_guard<std::mutex> lk(ws->mu);
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (prev != ws->device) cudaSetDevice(ws->device);
+    int s = ws_prepare(ws, a.g.ntiles, st);
+    if (!s) {
+        a.in = d_in;
+        a.out = d_out;
+        a.cap = cap;
+        a.ctl = ws->ctl;
+        a.state = ws->state;
+        a.epoch = ws->epoch;
+        a.sizes_out = reinterpret_cast<unsigned long long *>(d_sizes);
+        const bool pool = a.c.pool_min <= 64;
+        switch (vec_class(d_in, z, sizeof(T))) {
+        case 16: s = launch_enc_v<T, 16>(a, layout, pool, ws->sm_count, st); break;
+        case 4: s = launch_enc_v<T, 4>(a, layout, pool, ws->sm_count, st); break;
+        default:
+            if (sizeof(T) == 2) s = launch_enc_v<T, 2>(a, layout, pool, ws->sm_count, st);
+            else s = LSCOMP_ERR_ARG;
+            break;
+        }
+    }
+    if (prev != ws->device) cudaSetDevice(prev);
+    return s;
+}
+
+template <typename T>
+int compress_sync_t(lscomp_workspace *ws, const T *d_in, uint32_t x, uint32_t y, uint32_t z, const uint32_t bins[4],
+                    float pooling, uint8_t *d_out, uint64_t cap, uint64_t *stream_len, uint64_t *ref_size,
+                    void *stream)
+{
+    int s = compress_async_t<T>(ws, d_in, x, y, z, bins, pooling, d_out, cap, nullptr, stream);
+    if (s) return s;
+    std::lock_guard<std::mutex> lk(ws->mu);
+    s = read_ctl(ws, (cudaStream_t)stream);
+    if (s) return s;
+    uint64_t nb = (uint64_t)x * ((y + 7) / 8) * ((z + 7) / 8);
+    uint64_t total = ws->h_ctl->total;
+    if (sizeof(T) == 4) total &= 0xffffffffull;  // the reference reports a 32-bit total for uint32
+    if (stream_len) *stream_len = ws->h_ctl->stream_len;
+    if (ref_size) *ref_size = total + nb;
+    return LSCOMP_OK;
+}
+
+template <typename T>
+int decompress_async_t(lscomp_workspace *ws, const uint8_t *d_in, uint64_t cmp_len, uint32_t x, uint32_t y,
+                       uint32_t z, const uint32_t bins[4], float pooling, T *d_out, void *stream)
+{
+    if (!ws || !d_in || !d_out) return LSCOMP_ERR_ARG;
+    // the stream is read in 4-byte words
+    if (reinterpret_cast<uintptr_t>(d_out) % sizeof(T) || reinterpret_cast<uintptr_t>(d_in) % 4u) return LSCOMP_ERR_ARG;
+    DecArgs<T> a;
+    int layout = 0;
+    if (!make_geom(x, y, z, Elem<T>::kTileBlocks, a.g) || !make_codec(bins, pooling, sizeof(T) == 4, a.c, layout))
+        return LSCOMP_ERR_ARG;
+    if (cmp_len < a.g.nb) return LSCOMP_ERR_CAPACITY;
+    cudaStream_t st = (cudaStream_t)stream;
+    std::lock_guard<std::mutex> lk(ws->mu);
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (prev != ws->device) cudaSetDevice(ws->device);
+    int s = ws_prepare(ws, a.g.ntiles, st);
+    if (!s) {
+        a.in = d_in;
+        a.out = d_out;
+        a.cap = cmp_len;
+        a.ctl = ws->ctl;
+        a.state = ws->state;
+        a.tile_off = ws->state + ws->state_cap;
+        a.epoch = ws->epoch;
+        switch (vec_class(d_out, z, sizeof(T))) {
+        case 16: s = launch_dec_t<T, 16>(a, ws->sm_count, st); break;
+        case 4: s = launch_dec_t<T, 4>(a, ws->sm_count, st); break;
+        default:
+            if (sizeof(T) == 2) s = launch_dec_t<T, 2>(a, ws->sm_count, st);
+            else s = LSCOMP_ERR_ARG;
+            break;
+        }
+    }
+    if (prev != ws->device) cudaSetDevice(prev);
+    return s;
+}
+
 }  // namespace
+
 
 extern "C" {
 
@@ -238,6 +352,12 @@ uint64_t lscomp_max_stream_bytes_u16(uint32_t x, uint32_t y, uint32_t z)
 {
     uint64_t nb = lscomp_block_count(x, y, z);
     return (nb + 3) / 4 * 4 + 128ull * nb;
+}
+
+uint64_t lscomp_max_stream_bytes_u32(uint32_t x, uint32_t y, uint32_t z)
+{
+    uint64_t nb = lscomp_block_count(x, y, z);
+    return (nb + 3) / 4 * 4 + 248ull * nb;  // 31 planes of 8 bytes
 }
 
 uint64_t lscomp_launch_count(void) { return g_launches.load(); }
@@ -293,89 +413,57 @@ int lscomp_compress_u16_async(lscomp_workspace *ws, const uint16_t *d_in, uint32
                               const uint32_t bins[4], float pooling, uint8_t *d_out, uint64_t cap,
                               uint64_t *d_sizes, void *stream)
 {
-    if (!ws || !d_in || !d_out) return LSCOMP_ERR_ARG;
-    if (reinterpret_cast<uintptr_t>(d_in) & 1u) return LSCOMP_ERR_ARG;
-    EncArgs a;
-    int layout = 0;
-    if (!make_geom(x, y, z, a.g) || !make_codec(bins, pooling, a.c, layout)) return LSCOMP_ERR_ARG;
-    if (cap < a.g.R) return LSCOMP_ERR_CAPACITY;
-    cudaStream_t st = (cudaStream_t)stream;
-    std::lock_guard<std::mutex> lk(ws->mu);
-    int prev = 0;
-    cudaGetDevice(&prev);
-    if (prev != ws->device) cudaSetDevice(ws->device);
-    int s = ws_prepare(ws, a.g.ntiles, st);
-    if (!s) {
-        a.in = d_in;
-        a.out = d_out;
-        a.cap = cap;
-        a.ctl = ws->ctl;
-        a.state = ws->state;
-        a.epoch = ws->epoch;
-        a.sizes_out = reinterpret_cast<unsigned long long *>(d_sizes);
-        const bool pool = a.c.pool_min <= 64;
-        switch (vec_class(d_in, z)) {
-        case 16: s = launch_enc_v<16>(a, layout, pool, ws->sm_count, st); break;
-        case 4: s = launch_enc_v<4>(a, layout, pool, ws->sm_count, st); break;
-        default: s = launch_enc_v<2>(a, layout, pool, ws->sm_count, st); break;
-        }
-    }
-    if (prev != ws->device) cudaSetDevice(prev);
-    return s;
+    return compress_async_t<uint16_t>(ws, d_in, x, y, z, bins, pooling, d_out, cap, d_sizes, stream);
+}
+
+int lscomp_compress_u32_async(lscomp_workspace *ws, const uint32_t *d_in, uint32_t x, uint32_t y, uint32_t z,
+                              const uint32_t bins[4], float pooling, uint8_t *d_out, uint64_t cap,
+                              uint64_t *d_sizes, void *stream)
+{
+    return compress_async_t<uint32_t>(ws, d_in, x, y, z, bins, pooling, d_out, cap, d_sizes, stream);
 }
 
 int lscomp_compress_u16(lscomp_workspace *ws, const uint16_t *d_in, uint32_t x, uint32_t y, uint32_t z,
                         const uint32_t bins[4], float pooling, uint8_t *d_out, uint64_t cap,
                         uint64_t *stream_len, uint64_t *ref_size, void *stream)
 {
-    int s = lscomp_compress_u16_async(ws, d_in, x, y, z, bins, pooling, d_out, cap, nullptr, stream);
-    if (s) return s;
-    std::lock_guard<std::mutex> lk(ws->mu);
-    s = read_ctl(ws, (cudaStream_t)stream);
-    if (s) return s;
-    uint64_t nb = lscomp_block_count(x, y, z);
-    if (stream_len) *stream_len = ws->h_ctl->stream_len;
-    if (ref_size) *ref_size = ws->h_ctl->total + nb;
-    return LSCOMP_OK;
+    return compress_sync_t<uint16_t>(ws, d_in, x, y, z, bins, pooling, d_out, cap, stream_len, ref_size, stream);
+}
+
+int lscomp_compress_u32(lscomp_workspace *ws, const uint32_t *d_in, uint32_t x, uint32_t y, uint32_t z,
+                        const uint32_t bins[4], float pooling, uint8_t *d_out, uint64_t cap,
+                        uint64_t *stream_len, uint64_t *ref_size, void *stream)
+{
+    return compress_sync_t<uint32_t>(ws, d_in, x, y, z, bins, pooling, d_out, cap, stream_len, ref_size, stream);
 }
 
 int lscomp_decompress_u16_async(lscomp_workspace *ws, const uint8_t *d_in, uint64_t cmp_len, uint32_t x,
                                 uint32_t y, uint32_t z, const uint32_t bins[4], float pooling, uint16_t *d_out,
                                 void *stream)
 {
-    if (!ws || !d_in || !d_out) return LSCOMP_ERR_ARG;
-    if (reinterpret_cast<uintptr_t>(d_out) & 1u) return LSCOMP_ERR_ARG;
-    DecArgs a;
-    int layout = 0;
-    if (!make_geom(x, y, z, a.g) || !make_codec(bins, pooling, a.c, layout)) return LSCOMP_ERR_ARG;
-    if (cmp_len < a.g.nb) return LSCOMP_ERR_CAPACITY;
-    cudaStream_t st = (cudaStream_t)stream;
-    std::lock_guard<std::mutex> lk(ws->mu);
-    int prev = 0;
-    cudaGetDevice(&prev);
-    if (prev != ws->device) cudaSetDevice(ws->device);
-    int s = ws_prepare(ws, a.g.ntiles, st);
-    if (!s) {
-        a.in = d_in;
-        a.out = d_out;
-        a.cap = cmp_len;
-        a.ctl = ws->ctl;
-        a.state = ws->state;
-        a.epoch = ws->epoch;
-        switch (vec_class(d_out, z)) {
-        case 16: s = launch_dec_t<16>(a, ws->sm_count, st); break;
-        case 4: s = launch_dec_t<4>(a, ws->sm_count, st); break;
-        default: s = launch_dec_t<2>(a, ws->sm_count, st); break;
-        }
-    }
-    if (prev != ws->device) cudaSetDevice(prev);
-    return s;
+    return decompress_async_t<uint16_t>(ws, d_in, cmp_len, x, y, z, bins, pooling, d_out, stream);
+}
+
+int lscomp_decompress_u32_async(lscomp_workspace *ws, const uint8_t *d_in, uint64_t cmp_len, uint32_t x,
+                                uint32_t y, uint32_t z, const uint32_t bins[4], float pooling, uint32_t *d_out,
+                                void *stream)
+{
+    return decompress_async_t<uint32_t>(ws, d_in, cmp_len, x, y, z, bins, pooling, d_out, stream);
 }
 
 int lscomp_decompress_u16(lscomp_workspace *ws, const uint8_t *d_in, uint64_t cmp_len, uint32_t x, uint32_t y,
                           uint32_t z, const uint32_t bins[4], float pooling, uint16_t *d_out, void *stream)
 {
-    int s = lscomp_decompress_u16_async(ws, d_in, cmp_len, x, y, z, bins, pooling, d_out, stream);
+    int s = decompress_async_t<uint16_t>(ws, d_in, cmp_len, x, y, z, bins, pooling, d_out, stream);
+    if (s) return s;
+    std::lock_guard<std::mutex> lk(ws->mu);
+    return read_ctl(ws, (cudaStream_t)stream);
+}
+
+int lscomp_decompress_u32(lscomp_workspace *ws, const uint8_t *d_in, uint64_t cmp_len, uint32_t x, uint32_t y,
+                          uint32_t z, const uint32_t bins[4], float pooling, uint32_t *d_out, void *stream)
+{
+    int s = decompress_async_t<uint32_t>(ws, d_in, cmp_len, x, y, z, bins, pooling, d_out, stream);
     if (s) return s;
     std::lock_guard<std::mutex> lk(ws->mu);
     return read_ctl(ws, (cudaStream_t)stream);

@@ -1,29 +1,34 @@
-// codec_kernels.cuh -- the lsCOMP uint16 block codec as sm_100a kernels.
+// codec_kernels.cuh -- the lsCOMP block codec (uint16 and uint32 stacks) as
+// sm_100a kernels.
 //
 // One launch encodes (or decodes) a whole X x Y x Z stack (z fastest) in a
 // single pass over HBM:
 //
 //   * The stack is cut into *tiles* of consecutive 8x8 blocks (block index
 //     order = the stream's order, lsCOMP/src/cuLSZ_kernel.cu:868-872).  A tile
-//     is either G whole block-rows (when a block-row has <= kTileBlocks
-//     blocks; the tile's input is then one contiguous byte range) or one
-//     chunk of a single block-row (8 row segments).
+//     is either G whole block-rows (when a block-row has at most
+//     Elem<T>::kTileBlocks blocks; the tile's input is then one contiguous
+//     byte range) or one chunk of a single block-row (8 row segments).
 //   * Persistent CTAs claim tiles in increasing order from a ticket counter,
 //     so every tile a CTA waits on in the scan belongs to a resident CTA.
-//   * Encoder: a tile's input is fetched once with 1-D TMA bulk copies into a
-//     double-buffered shared-memory stage; per-block statistics, pooling, bin
-//     choice and rate come from one pass over the stage; the tile's payload
-//     size is published, a warp-wide decoupled look-back yields the tile's
-//     stream offset, and the bit planes are packed from shared memory
-//     straight to their final place in the stream.
-//   * Decoder: header bytes -> sizes -> the same look-back -> plane words
-//     gathered per block -> values scattered to the output rows.
+//   * Encoder (one CTA per SM, warp-specialised): a producer warp fetches
+//     each tile's input once with 1-D TMA bulk copies into a 3-deep ring;
+//     16 compute warps take the rows into registers, derive every block's
+//     statistics, pooling, bin choice and rate, publish the tile's payload
+//     size and pack the bit planes into a 3-deep payload ring; a writer warp
+//     runs the decoupled look-back for the tile's stream offset and copies
+//     the packed payload to the stream.  Only the writer waits on other
+//     CTAs, and the compute warps run up to three tiles ahead of it.
+//   * Decoder: a small kernel turns the header bytes into per-tile stream
+//     offsets; the decode kernel then handles every tile independently
+//     (plane words gathered per block, values scattered to the rows).
 //
 // Thread layout inside a warp ("unit" = 8 consecutive blocks of a tile):
 // lane = j + 8 r, j = block within the unit, r = 0..3; the lane owns rows r
-// and r+4 of block j (8 values each, held as 4 words of two uint16).  The 4
-// lanes of a block sit 8 lanes apart, so block reductions and the 4x4 byte
-// transposes that assemble plane words are two xor-shuffles (8, 16).
+// and r+4 of block j (8 values each, held as a Row: 4 words of two uint16, or
+// 8 words of one uint32).  The 4 lanes of a block sit 8 lanes apart, so block
+// reductions and the 4x4 byte transposes that assemble plane words are two
+// xor-shuffles (8, 16).
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -32,18 +37,35 @@
 
 namespace lsc {
 
-constexpr int kThreads = 256;                     // 8 warps per CTA
+constexpr int kThreads = 256;                  // 8 warps per CTA
 constexpr int kWarps = kThreads / 32;
-constexpr int kTileBlocks = 256;                  // at most this many blocks per tile
-constexpr int kUnitsPerTile = kTileBlocks / 8;
-constexpr int kChunkPitch = kTileBlocks * 16 + 32; // bytes per row segment (chunk tiles)
-constexpr int kStageBytes = 33280;                // >= one tile's input + alignment slack
-constexpr int kStages = 2;
+constexpr int kMaxTileBlocks = 256;            // smem tables are sized for this
+constexpr int kChunkPitch = 4096 + 32;         // bytes per row segment (chunk tiles)
+constexpr int kStageBytes = 33280;             // >= one tile's input + alignment slack
 
 // bins layouts (template parameter)
 constexpr int BINS_EQUAL = 0;   // all four bins equal: bin choice is always 3
 constexpr int BINS_MONO = 1;    // x <= y <= z <= w (what the CLI accepts)
 constexpr int BINS_GENERAL = 2; // anything else the host API allows
+
+// Per element type: words per 8-value row, plane byte groups, largest rate
+// the 5-bit header field carries, and blocks per tile (4 KB of input per
+// row segment for both types).
+template <typename T> struct Elem;
+template <> struct Elem<uint16_t> {
+    static constexpr int kWords = 4;
+    static constexpr int kGroups = 2;
+    static constexpr uint32_t kMaxRate = 16;
+    static constexpr int kTileBlocks = 256;
+};
+template <> struct Elem<uint32_t> {
+    static constexpr int kWords = 8;
+    static constexpr int kGroups = 4;
+    static constexpr uint32_t kMaxRate = 31;
+    static constexpr int kTileBlocks = 128;
+};
+
+template <typename T> struct Row { uint32_t w[Elem<T>::kWords]; };
 
 struct Geom {
     uint32_t X, Y, Z;
@@ -61,15 +83,17 @@ struct Geom {
 
 struct Codec {
     uint32_t bins[4];
-    uint32_t magic[4];   // ceil(2^32 / bin) for bin >= 2, 0 for bin == 1 (identity)
-    uint32_t binc[4];    // bins clamped to 65536 (same counts for 16-bit values)
-    int pool_min;        // a block pools iff zero count >= pool_min (65: never)
+    uint32_t magic[4];             // uint16: ceil(2^32 / bin) for bin >= 2, 0 for bin == 1
+    unsigned long long magic64[4]; // uint32: ceil(2^64 / bin) for bin >= 2, 0 for bin == 1
+    uint32_t binc[4];              // bins for the comparisons (uint16: clamped to 65536)
+    int pool_min;                  // a block pools iff zero count >= pool_min (65: never)
 };
 
+template <typename T>
 struct EncArgs {
     Geom g;
     Codec c;
-    const uint16_t *in;
+    const T *in;
     uint8_t *out;
     unsigned long long cap;
     LaunchCtl *ctl;
@@ -78,14 +102,16 @@ struct EncArgs {
     unsigned long long *sizes_out;  // optional device copy of {stream_len, payload}
 };
 
+template <typename T>
 struct DecArgs {
     Geom g;
     Codec c;
     const uint8_t *in;
-    uint16_t *out;
+    T *out;
     unsigned long long cap;  // readable stream bytes
     LaunchCtl *ctl;
-    unsigned long long *state;
+    unsigned long long *state;    // look-back state of the offsets kernel (per segment)
+    unsigned long long *tile_off; // per-tile payload offsets
     uint32_t epoch;
 };
 
@@ -132,49 +158,83 @@ __device__ __forceinline__ unsigned long long brow_start(const Geom &g, unsigned
 }
 
 // ---------------------------------------------------------------- row I/O
-// Load 8 uint16 at p (alignment VEC bytes) as 4 packed words.
+// Load the 8 values at p (alignment VEC bytes).
 template <int VEC>
-__device__ __forceinline__ void load8(const uint8_t *p, uint32_t w[4])
+__device__ __forceinline__ void load8(const uint8_t *p, Row<uint16_t> &v)
 {
     if (VEC == 16) {
-        uint4 v = *reinterpret_cast<const uint4 *>(p);
-        w[0] = v.x; w[1] = v.y; w[2] = v.z; w[3] = v.w;
+        uint4 q = *reinterpret_cast<const uint4 *>(p);
+        v.w[0] = q.x; v.w[1] = q.y; v.w[2] = q.z; v.w[3] = q.w;
     } else if (VEC == 4) {
         const uint32_t *q = reinterpret_cast<const uint32_t *>(p);
-        w[0] = q[0]; w[1] = q[1]; w[2] = q[2]; w[3] = q[3];
+        v.w[0] = q[0]; v.w[1] = q[1]; v.w[2] = q[2]; v.w[3] = q[3];
     } else {
         const uint16_t *h = reinterpret_cast<const uint16_t *>(p);
 #pragma unroll
-        for (int i = 0; i < 4; i++) w[i] = (uint32_t)h[2 * i] | ((uint32_t)h[2 * i + 1] << 16);
+        for (int i = 0; i < 4; i++) v.w[i] = (uint32_t)h[2 * i] | ((uint32_t)h[2 * i + 1] << 16);
+    }
+}
+
+template <int VEC>
+__device__ __forceinline__ void load8(const uint8_t *p, Row<uint32_t> &v)
+{
+    if (VEC == 16) {
+        uint4 a = reinterpret_cast<const uint4 *>(p)[0], b = reinterpret_cast<const uint4 *>(p)[1];
+        v.w[0] = a.x; v.w[1] = a.y; v.w[2] = a.z; v.w[3] = a.w;
+        v.w[4] = b.x; v.w[5] = b.y; v.w[6] = b.z; v.w[7] = b.w;
+    } else {
+        const uint32_t *q = reinterpret_cast<const uint32_t *>(p);
+#pragma unroll
+        for (int i = 0; i < 8; i++) v.w[i] = q[i];
     }
 }
 
 // keep only the first ncols (1..8) values
-__device__ __forceinline__ void mask_cols(uint32_t w[4], uint32_t ncols)
+__device__ __forceinline__ void mask_cols(Row<uint16_t> &v, uint32_t ncols)
 {
 #pragma unroll
     for (int i = 0; i < 4; i++) {
         uint32_t keep = ncols >= 2u * i + 2u ? 0xffffffffu : (ncols == 2u * i + 1u ? 0x0000ffffu : 0u);
-        w[i] &= keep;
+        v.w[i] &= keep;
     }
 }
 
+__device__ __forceinline__ void mask_cols(Row<uint32_t> &v, uint32_t ncols)
+{
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+        if ((uint32_t)i >= ncols) v.w[i] = 0;
+}
+
 template <int VEC>
-__device__ __forceinline__ void store8(uint16_t *p, const uint32_t w[4], uint32_t ncols)
+__device__ __forceinline__ void store8(uint16_t *p, const Row<uint16_t> &v, uint32_t ncols)
 {
     if (ncols >= 8u) {
         if (VEC == 16) {
-            *reinterpret_cast<uint4 *>(p) = make_uint4(w[0], w[1], w[2], w[3]);
+            *reinterpret_cast<uint4 *>(p) = make_uint4(v.w[0], v.w[1], v.w[2], v.w[3]);
             return;
         } else if (VEC == 4) {
             uint32_t *q = reinterpret_cast<uint32_t *>(p);
-            q[0] = w[0]; q[1] = w[1]; q[2] = w[2]; q[3] = w[3];
+            q[0] = v.w[0]; q[1] = v.w[1]; q[2] = v.w[2]; q[3] = v.w[3];
             return;
         }
     }
 #pragma unroll
     for (int i = 0; i < 8; i++)
-        if ((uint32_t)i < ncols) p[i] = (uint16_t)(w[i >> 1] >> (16 * (i & 1)));
+        if ((uint32_t)i < ncols) p[i] = (uint16_t)(v.w[i >> 1] >> (16 * (i & 1)));
+}
+
+template <int VEC>
+__device__ __forceinline__ void store8(uint32_t *p, const Row<uint32_t> &v, uint32_t ncols)
+{
+    if (ncols >= 8u && VEC == 16) {
+        reinterpret_cast<uint4 *>(p)[0] = make_uint4(v.w[0], v.w[1], v.w[2], v.w[3]);
+        reinterpret_cast<uint4 *>(p)[1] = make_uint4(v.w[4], v.w[5], v.w[6], v.w[7]);
+        return;
+    }
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+        if ((uint32_t)i < ncols) p[i] = v.w[i];
 }
 
 // ---------------------------------------------------------------- arithmetic
@@ -185,7 +245,59 @@ __device__ __forceinline__ uint32_t zero_halves(uint32_t w)
     return 2u - __popc(t & 0x80008000u);
 }
 
-// quantise both halves of w by the bin whose magic number is m (0 = bin 1)
+__device__ __forceinline__ uint32_t zeros(const Row<uint16_t> &v)
+{
+    return zero_halves(v.w[0]) + zero_halves(v.w[1]) + zero_halves(v.w[2]) + zero_halves(v.w[3]);
+}
+
+__device__ __forceinline__ uint32_t zeros(const Row<uint32_t> &v)
+{
+    uint32_t z = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) z += v.w[i] == 0u;
+    return z;
+}
+
+// min over the row of (value - b0) mod 2^32
+__device__ __forceinline__ uint32_t min_from(const Row<uint16_t> &v, uint32_t b0, uint32_t mn)
+{
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        mn = min(mn, (v.w[i] & 0xffffu) - b0);
+        mn = min(mn, (v.w[i] >> 16) - b0);
+    }
+    return mn;
+}
+
+__device__ __forceinline__ uint32_t min_from(const Row<uint32_t> &v, uint32_t b0, uint32_t mn)
+{
+#pragma unroll
+    for (int i = 0; i < 8; i++) mn = min(mn, v.w[i] - b0);
+    return mn;
+}
+
+__device__ __forceinline__ uint32_t value_at(const Row<uint16_t> &v, int i)
+{
+    return (v.w[i >> 1] >> (16 * (i & 1))) & 0xffffu;
+}
+
+__device__ __forceinline__ uint32_t value_at(const Row<uint32_t> &v, int i) { return v.w[i]; }
+
+// four 8-bit counters of (value < binc[k])
+template <typename T>
+__device__ __forceinline__ uint32_t bin_counts(const Row<T> &v, const uint32_t *binc)
+{
+    uint32_t cnt = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        uint32_t x = value_at(v, i);
+        cnt += (uint32_t)(x < binc[0]) | ((uint32_t)(x < binc[1]) << 8) | ((uint32_t)(x < binc[2]) << 16) |
+               ((uint32_t)(x < binc[3]) << 24);
+    }
+    return cnt;
+}
+
+// quantise every value of the row by the chosen bin
 __device__ __forceinline__ uint32_t quant2(uint32_t w, uint32_t m)
 {
     if (m == 0u) return w;
@@ -194,19 +306,137 @@ __device__ __forceinline__ uint32_t quant2(uint32_t w, uint32_t m)
     return lo | (hi << 16);
 }
 
-// pooled values of one row: floor((v[2p] + v[2p+1]) / 2), p = 0..3, packed
-// as two words (p0 | p1 << 16, p2 | p3 << 16)
-__device__ __forceinline__ void pool_row(const uint32_t w[4], uint32_t &a, uint32_t &b)
+__device__ __forceinline__ void quant(Row<uint16_t> &v, const Codec &c, uint32_t choice)
 {
-    uint32_t m0 = ((w[0] & 0xffffu) + (w[0] >> 16)) >> 1;
-    uint32_t m1 = ((w[1] & 0xffffu) + (w[1] >> 16)) >> 1;
-    uint32_t m2 = ((w[2] & 0xffffu) + (w[2] >> 16)) >> 1;
-    uint32_t m3 = ((w[3] & 0xffffu) + (w[3] >> 16)) >> 1;
-    a = m0 | (m1 << 16);
-    b = m2 | (m3 << 16);
+    const uint32_t m = c.magic[choice];
+#pragma unroll
+    for (int i = 0; i < 4; i++) v.w[i] = quant2(v.w[i], m);
+}
+
+__device__ __forceinline__ void quant(Row<uint32_t> &v, const Codec &c, uint32_t choice)
+{
+    const unsigned long long m = c.magic64[choice];
+    if (m == 0ull) return;
+#pragma unroll
+    for (int i = 0; i < 8; i++) v.w[i] = (uint32_t)__umul64hi((unsigned long long)v.w[i], m);
+}
+
+// pooled values of rows a and b: floor((v[2p] + v[2p+1]) / 2) with the sum
+// in 32-bit unsigned arithmetic (lsCOMP/src/cuLSZ_kernel.cu:914,1109); the 4
+// of row a then the 4 of row b, as one Row
+__device__ __forceinline__ Row<uint16_t> pool_rows(const Row<uint16_t> &a, const Row<uint16_t> &b)
+{
+    Row<uint16_t> p;
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+        const Row<uint16_t> &s = i ? b : a;
+        uint32_t m0 = ((s.w[0] & 0xffffu) + (s.w[0] >> 16)) >> 1;
+        uint32_t m1 = ((s.w[1] & 0xffffu) + (s.w[1] >> 16)) >> 1;
+        uint32_t m2 = ((s.w[2] & 0xffffu) + (s.w[2] >> 16)) >> 1;
+        uint32_t m3 = ((s.w[3] & 0xffffu) + (s.w[3] >> 16)) >> 1;
+        p.w[2 * i] = m0 | (m1 << 16);
+        p.w[2 * i + 1] = m2 | (m3 << 16);
+    }
+    return p;
+}
+
+__device__ __forceinline__ Row<uint32_t> pool_rows(const Row<uint32_t> &a, const Row<uint32_t> &b)
+{
+    Row<uint32_t> p;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        p.w[i] = (a.w[2 * i] + a.w[2 * i + 1]) >> 1;  // the sum wraps, as in the reference
+        p.w[4 + i] = (b.w[2 * i] + b.w[2 * i + 1]) >> 1;
+    }
+    return p;
+}
+
+__device__ __forceinline__ uint32_t or_all(const Row<uint16_t> &v)
+{
+    uint32_t o = v.w[0] | v.w[1] | v.w[2] | v.w[3];
+    return (o & 0xffffu) | (o >> 16);
+}
+
+__device__ __forceinline__ uint32_t or_all(const Row<uint32_t> &v)
+{
+    uint32_t o = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) o |= v.w[i];
+    return o;
 }
 
 __device__ __forceinline__ uint32_t bitlen(uint32_t v) { return 32u - __clz(v); }
+
+// plane bytes of byte group g (planes 8g..8g+7) of one row: on return lo holds
+// planes 8g+{0,1,2,3} and hi planes 8g+{4,5,6,7}, one byte per plane
+__device__ __forceinline__ void row_planes(const Row<uint16_t> &v, uint32_t g, uint32_t &lo, uint32_t &hi)
+{
+    lsc_row_planes(v.w[0], v.w[1], v.w[2], v.w[3], (int)g, lo, hi);
+}
+
+__device__ __forceinline__ void row_planes(const Row<uint32_t> &v, uint32_t g, uint32_t &lo, uint32_t &hi)
+{
+    const uint32_t s2 = g | ((g + 4u) << 4);  // byte g of the first, byte g of the second word
+    lo = __byte_perm(__byte_perm(v.w[7], v.w[6], s2), __byte_perm(v.w[5], v.w[4], s2), 0x5410u);
+    hi = __byte_perm(__byte_perm(v.w[3], v.w[2], s2), __byte_perm(v.w[1], v.w[0], s2), 0x5410u);
+    lsc_transpose8x8(lo, hi);
+}
+
+// inverse of row_planes over all groups: P[g][0] = lo, P[g][1] = hi
+__device__ __forceinline__ void row_values(uint32_t P[][2], Row<uint16_t> &v)
+{
+    lsc_row_values(P[0][0], P[0][1], P[1][0], P[1][1], v.w[0], v.w[1], v.w[2], v.w[3]);
+}
+
+__device__ __forceinline__ void row_values(uint32_t P[][2], Row<uint32_t> &v)
+{
+#pragma unroll
+    for (int g = 0; g < 4; g++) lsc_transpose8x8(P[g][0], P[g][1]);  // byte g of v7..v4 / v3..v0
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const uint32_t s = (uint32_t)k | ((uint32_t)(k + 4) << 4);
+        v.w[7 - k] = __byte_perm(__byte_perm(P[0][0], P[1][0], s), __byte_perm(P[2][0], P[3][0], s), 0x5410u);
+        v.w[3 - k] = __byte_perm(__byte_perm(P[0][1], P[1][1], s), __byte_perm(P[2][1], P[3][1], s), 0x5410u);
+    }
+}
+
+__device__ __forceinline__ void dequant(Row<uint16_t> &v, uint32_t bin)
+{
+    if (bin == 1u) return;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        uint32_t lo = (v.w[i] & 0xffffu) * bin, hi = (v.w[i] >> 16) * bin;
+        v.w[i] = (lo & 0xffffu) | (hi << 16);
+    }
+}
+
+__device__ __forceinline__ void dequant(Row<uint32_t> &v, uint32_t bin)
+{
+#pragma unroll
+    for (int i = 0; i < 8; i++) v.w[i] *= bin;
+}
+
+// one output row from 4 pooled quantised values (the first half of q, or
+// the second): each value de-quantised and repeated over its two columns
+__device__ __forceinline__ Row<uint16_t> unpool_row(const Row<uint16_t> &q, bool second, uint32_t bin)
+{
+    Row<uint16_t> v;
+    const uint32_t a = q.w[second ? 2 : 0], b = q.w[second ? 3 : 1];
+    uint32_t x0 = (a & 0xffffu) * bin, x1 = (a >> 16) * bin, x2 = (b & 0xffffu) * bin, x3 = (b >> 16) * bin;
+    v.w[0] = (x0 & 0xffffu) | (x0 << 16);
+    v.w[1] = (x1 & 0xffffu) | (x1 << 16);
+    v.w[2] = (x2 & 0xffffu) | (x2 << 16);
+    v.w[3] = (x3 & 0xffffu) | (x3 << 16);
+    return v;
+}
+
+__device__ __forceinline__ Row<uint32_t> unpool_row(const Row<uint32_t> &q, bool second, uint32_t bin)
+{
+    Row<uint32_t> v;
+#pragma unroll
+    for (int i = 0; i < 4; i++) v.w[2 * i] = v.w[2 * i + 1] = q.w[(second ? 4 : 0) + i] * bin;
+    return v;
+}
 
 // 4x4 byte transpose across the lanes j, j+8, j+16, j+24 (r = lane >> 3):
 // lane r ends with byte c = byte r of lane c's input.
@@ -219,28 +449,44 @@ __device__ __forceinline__ uint32_t xpose4(uint32_t x, uint32_t r)
 }
 
 // ---------------------------------------------------------------- shared state
+// Encoder CTA: kEncWarps compute warps, one producer warp (tile claims and
+// TMA loads) and one writer warp (look-back and write-out), one CTA per SM.
+constexpr int kEncWarps = 16;
+constexpr int kEncThreads = (kEncWarps + 2) * 32;
+constexpr int kProducerWarp = kEncWarps;
+constexpr int kWriterWarp = kEncWarps + 1;
+constexpr int kInStages = 3;                  // input ring (TMA destination)
+constexpr int kStStages = 3;                  // packed-payload ring (write-out source)
+constexpr int kStagingBytes = 32896;          // >= one tile's worst-case payload (32768)
+constexpr uint32_t kComputeBarrier = 1;       // named barrier of the compute warps
+
 struct EncSmem {
-    alignas(128) uint8_t stage[kStages][kStageBytes];
-    uint64_t bar[kStages];
-    unsigned long long tile[kStages];
-    uint32_t mis[kStages][8];       // byte misalignment of each range start (mod 16)
-    uint32_t br_rel[kTileBlocks];   // whole-row tiles: element offset of block-row g from the tile start
-    uint8_t br_rows[kTileBlocks];   // rows in block-row g
-    uint8_t hdr[kTileBlocks];       // header byte per block
-    uint32_t off[kTileBlocks];      // payload offset of each block inside the tile
-    unsigned long long base;        // stream offset of the tile payload (relative to R)
+    alignas(128) uint8_t in[kInStages][kStageBytes];
+    alignas(128) uint8_t st[kStStages][kStagingBytes];
+    uint64_t in_full[kInStages];       // producer -> compute: tile input landed
+    uint64_t in_empty[kInStages];      // compute -> producer: input slot read
+    uint64_t st_full[kStStages];       // compute -> writer: payload packed
+    uint64_t st_empty[kStStages];      // writer -> compute: payload written out
+    unsigned long long in_tile[kInStages];
+    uint32_t in_mis[kInStages][8];     // byte misalignment of each range start (mod 16)
+    unsigned long long st_tile[kStStages];
+    uint32_t st_agg[kStStages];
+    uint32_t br_rel[kMaxTileBlocks];   // whole-row tiles: element offset of block-row g from the tile start
+    uint8_t br_rows[kMaxTileBlocks];   // rows in block-row g
+    uint8_t hdr[kMaxTileBlocks];       // header byte per block
+    uint32_t off[kMaxTileBlocks];      // payload offset of each block inside the tile
     uint32_t agg;
-    uint32_t flag_ok;
+    uint32_t range_err;
+    uint32_t consumed;                 // input-ring entries the compute warps took
+    uint32_t issued;                   // input-ring entries the producer filled
 };
 
 struct DecSmem {
-    unsigned long long tile;
-    uint32_t br_rel[kTileBlocks];
-    uint8_t br_rows[kTileBlocks];
-    uint8_t hdr[kTileBlocks];
-    uint32_t off[kTileBlocks];
+    uint32_t br_rel[kMaxTileBlocks];
+    uint8_t br_rows[kMaxTileBlocks];
+    uint8_t hdr[kMaxTileBlocks];
+    uint32_t off[kMaxTileBlocks];
     unsigned long long base;
-    uint32_t agg;
     uint32_t flag_ok;
 };
 
@@ -294,20 +540,21 @@ __device__ __forceinline__ unsigned long long tile_prefix(unsigned long long *st
 
 // ---------------------------------------------------------------- encoder
 // Thread 0: claim-time bookkeeping and TMA issue for one tile into stage s.
-template <int VEC>
-__device__ void enc_issue(const EncArgs &a, EncSmem &sm, int s, unsigned long long t)
+template <typename T>
+__device__ void enc_issue(const EncArgs<T> &a, EncSmem &sm, int s, unsigned long long t)
 {
-    sm.tile[s] = t;
+    sm.in_tile[s] = t;
     if (t >= a.g.ntiles) {
-        mbar_arrive(&sm.bar[s]);
+        mbar_arrive(&sm.in_full[s]);
         return;
     }
+    constexpr uint32_t ES = sizeof(T);
     const Geom &g = a.g;
     TileInfo ti = tile_info(g, t);
     const uintptr_t base = reinterpret_cast<uintptr_t>(a.in);
     const uintptr_t A0 = (base + 15) & ~(uintptr_t)15;
-    const uintptr_t A1 = (base + 2ull * g.N) & ~(uintptr_t)15;
-    uint8_t *stage = sm.stage[s];
+    const uintptr_t A1 = (base + ES * g.N) & ~(uintptr_t)15;
+    uint8_t *stage = sm.in[s];
 
     // ranges: whole-row tiles -> 1 contiguous range; chunked -> one per row
     uint32_t nr;
@@ -336,43 +583,44 @@ __device__ void enc_issue(const EncArgs &a, EncSmem &sm, int s, unsigned long lo
     uint8_t *dst_[8];
     for (uint32_t i = 0; i < nr; i++) {
         uint8_t *sb = stage + (g.chunked ? i * kChunkPitch : 0);
-        uintptr_t ga = base + 2ull * es[i];
-        uintptr_t ge = ga + 2ull * ne[i];
+        uintptr_t ga = base + ES * es[i];
+        uintptr_t ge = ga + ES * ne[i];
         uintptr_t gs = ga & ~(uintptr_t)15;
-        sm.mis[s][i] = (uint32_t)(ga & 15);
+        sm.in_mis[s][i] = (uint32_t)(ga & 15);
         uintptr_t cs = gs > A0 ? gs : A0;
         uintptr_t ce = (ge + 15) & ~(uintptr_t)15;
         if (ce > A1) ce = A1;
         cs_[i] = cs; ce_[i] = ce; dst_[i] = sb + (cs - gs);
         if (ce > cs) tx += (uint32_t)(ce - cs);
         // bytes outside the 16-byte-aligned interior of the whole array
-        // (only the first and last tiles): copy them as 16-bit values
-        for (uintptr_t p = ga; p < ge && p < A0; p += 2)
-            *reinterpret_cast<uint16_t *>(sb + (p - gs)) = *reinterpret_cast<const uint16_t *>(p);
-        for (uintptr_t p = (ga > A1 ? ga : A1); p < ge; p += 2)
-            *reinterpret_cast<uint16_t *>(sb + (p - gs)) = *reinterpret_cast<const uint16_t *>(p);
+        // (only the first and last tiles): copy them element by element
+        for (uintptr_t p = ga; p < ge && p < A0; p += ES)
+            *reinterpret_cast<T *>(sb + (p - gs)) = *reinterpret_cast<const T *>(p);
+        for (uintptr_t p = (ga > A1 ? ga : A1); p < ge; p += ES)
+            *reinterpret_cast<T *>(sb + (p - gs)) = *reinterpret_cast<const T *>(p);
     }
     fence_proxy_async_smem();
-    mbar_arrive_expect_tx(&sm.bar[s], tx);
+    mbar_arrive_expect_tx(&sm.in_full[s], tx);
     for (uint32_t i = 0; i < nr; i++)
         if (ce_[i] > cs_[i])
-            bulk_g2s(dst_[i], reinterpret_cast<const void *>(cs_[i]), (uint32_t)(ce_[i] - cs_[i]), &sm.bar[s]);
+            bulk_g2s(dst_[i], reinterpret_cast<const void *>(cs_[i]), (uint32_t)(ce_[i] - cs_[i]), &sm.in_full[s]);
 }
 
-// Where lane's two row segments (rows r and r+4 of tile-local block b) live
-// in the stage, and how many rows / columns of the block are real.
+// Where a lane's two row segments (rows r and r+4 of tile-local block b)
+// live, and how many rows / columns of the block are real.
 struct SegLoc {
     const uint8_t *pA, *pB;
     uint32_t nrows, ncols;
     uint32_t bz;
-    unsigned long long growA;  // global row index of row r (decoder)
+    unsigned long long growA;  // element offset of row r's segment from the tile's first row (decoder)
 };
 
-template <bool ENC>
+template <typename T, bool ENC>
 __device__ __forceinline__ SegLoc seg_locate(const Geom &g, const TileInfo &ti, const uint32_t *br_rel,
                                              const uint8_t *br_rows, const uint8_t *stage, const uint32_t *mis,
                                              uint32_t b, uint32_t r)
 {
+    constexpr uint32_t ES = sizeof(T);
     SegLoc L;
     if (!g.chunked) {
         uint32_t gidx = (b * g.inv_bzb) >> 16;
@@ -380,16 +628,16 @@ __device__ __forceinline__ SegLoc seg_locate(const Geom &g, const TileInfo &ti, 
         L.nrows = br_rows[gidx];
         unsigned long long e = (unsigned long long)br_rel[gidx] + (unsigned long long)r * g.Z + 8ull * L.bz;
         if (ENC) {
-            L.pA = stage + mis[0] + 2ull * e;
-            L.pB = L.pA + 8ull * g.Z;
+            L.pA = stage + mis[0] + ES * e;
+            L.pB = L.pA + 4ull * ES * g.Z;
         }
-        L.growA = e;  // relative element offset (decoder adds the tile start)
+        L.growA = e;
     } else {
         L.bz = ti.c0 + b;
         L.nrows = br_rows[0];
         if (ENC) {
-            L.pA = stage + r * kChunkPitch + mis[r] + 16u * b;
-            L.pB = stage + (r + 4) * kChunkPitch + mis[(r + 4) & 7] + 16u * b;
+            L.pA = stage + r * kChunkPitch + mis[r] + 8u * ES * b;
+            L.pB = stage + (r + 4) * kChunkPitch + mis[(r + 4) & 7] + 8u * ES * b;
         }
         L.growA = (unsigned long long)r * g.Z + 8ull * L.bz;
     }
@@ -398,45 +646,195 @@ __device__ __forceinline__ SegLoc seg_locate(const Geom &g, const TileInfo &ti, 
     return L;
 }
 
-template <int VEC, int BINS, bool POOL>
-__global__ void __launch_bounds__(kThreads, 2) enc_kernel(const EncArgs a)
+template <typename T, int VEC>
+__device__ __forceinline__ void load_rows(const SegLoc &L, bool active, uint32_t r, Row<T> &A, Row<T> &B)
 {
-    extern __shared__ __align__(128) uint8_t smem_raw[];
-    EncSmem &sm = *reinterpret_cast<EncSmem *>(smem_raw);
+#pragma unroll
+    for (int i = 0; i < Elem<T>::kWords; i++) A.w[i] = B.w[i] = 0;
+    if (active && r < L.nrows) {
+        load8<VEC>(L.pA, A);
+        if (L.ncols < 8) mask_cols(A, L.ncols);
+    }
+    if (active && r + 4 < L.nrows) {
+        load8<VEC>(L.pB, B);
+        if (L.ncols < 8) mask_cols(B, L.ncols);
+    }
+}
+
+__device__ __forceinline__ void compute_bar() { asm volatile("bar.sync %0, %1;" ::"r"(kComputeBarrier), "r"(kEncWarps * 32) : "memory"); }
+
+__device__ __forceinline__ bool compute_bar_and(bool pred)
+{
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.and.pred q, %2, %3, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)pred), "r"(kComputeBarrier), "r"(kEncWarps * 32)
+        : "memory");
+    return r != 0;
+}
+
+// Pass A for one unit: statistics -> header byte (lsCOMP/src/cuLSZ_kernel.cu:898-957).
+// Returns the header byte (same in the 4 lanes of a block).
+template <typename T, int BINS, bool POOL>
+__device__ __forceinline__ uint32_t block_header(const Row<T> &A, const Row<T> &B, const Codec &c, uint32_t &range_bad)
+{
+    uint32_t choice = 3;
+    if (BINS == BINS_MONO) {
+        // the bin counts of cuLSZ_kernel.cu:906-935 are equal exactly when no
+        // value lies between the two bins, so the choice is the interval
+        // holding the smallest value >= bin0
+        const uint32_t b0 = c.binc[0];
+        uint32_t mn = min_from(B, b0, min_from(A, b0, 0xffffffffu));
+        mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, 8));
+        mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, 16));
+        const uint32_t v = mn + b0;  // smallest value >= bin0 (if any)
+        const bool any = sizeof(T) == 2 ? (mn < 0x80000000u) : (mn <= ~b0);
+        choice = (any && v < c.binc[1])   ? 0u
+                 : (any && v < c.binc[2]) ? 1u
+                 : (any && v < c.binc[3]) ? 2u
+                                          : 3u;
+    } else if (BINS == BINS_GENERAL) {
+        uint32_t cnt = bin_counts(A, c.binc) + bin_counts(B, c.binc);
+        cnt += __shfl_xor_sync(0xffffffffu, cnt, 8);
+        cnt += __shfl_xor_sync(0xffffffffu, cnt, 16);
+        const uint32_t c0 = cnt & 0xff, c1 = (cnt >> 8) & 0xff, c2 = (cnt >> 16) & 0xff, c3 = cnt >> 24;
+        choice = 0;
+        if (c1 == c0) {
+            choice = 1;
+            if (c2 == c1) {
+                choice = 2;
+                if (c3 == c2) choice = 3;
+            }
+        }
+    }
+    bool pool = false;
+    if (POOL) {
+        uint32_t zc = zeros(A) + zeros(B);
+        zc += __shfl_xor_sync(0xffffffffu, zc, 8);
+        zc += __shfl_xor_sync(0xffffffffu, zc, 16);
+        pool = (int)zc >= c.pool_min;
+    }
+    uint32_t orv;
+    if (pool) {
+        Row<T> P = pool_rows(A, B);
+        quant(P, c, choice);
+        orv = or_all(P);
+    } else {
+        Row<T> qa = A, qb = B;
+        quant(qa, c, choice);
+        quant(qb, c, choice);
+        orv = or_all(qa) | or_all(qb);
+    }
+    orv |= __shfl_xor_sync(0xffffffffu, orv, 8);
+    orv |= __shfl_xor_sync(0xffffffffu, orv, 16);
+    const uint32_t rate = bitlen(orv);
+    range_bad = rate > Elem<T>::kMaxRate;
+    return (pool ? 0x80u : 0u) | (choice << 5) | (rate & 0x1fu);
+}
+
+// Pass B for one unit: bit planes (lsCOMP/src/cuLSZ_kernel.cu:1100-1276) of
+// the block whose header is h, stored at dst (shared memory).
+template <typename T>
+__device__ __forceinline__ void block_pack(const Row<T> &A0, const Row<T> &B0, uint32_t h, bool active, uint32_t r,
+                                           const Codec &c, uint8_t *dst)
+{
+    constexpr int NW = Elem<T>::kWords;
+    constexpr int NG = Elem<T>::kGroups;
+    const bool even = (r & 1u) == 0;
+    const bool pool = (h & 0x80u) != 0;
+    const uint32_t rate = h & 0x1fu;
+    const uint32_t choice = (h >> 5) & 3u;
+    Row<T> A = A0, B = B0;
+    if (__any_sync(0xffffffffu, active && pool)) {
+        // pooled blocks: lane r=0 takes row pair (0,1), r=1 (4,5), r=2 (2,3),
+        // r=3 (6,7) -- one pooled byte row each
+        Row<T> P = pool_rows(A0, B0);
+        quant(P, c, choice);
+        Row<T> V;
+#pragma unroll
+        for (int i = 0; i < NW / 2; i++) {
+            // even lanes send their second row, odd lanes their first
+            const uint32_t t0 = __shfl_xor_sync(0xffffffffu, even ? P.w[NW / 2 + i] : P.w[i], 8);
+            V.w[i] = even ? P.w[i] : t0;
+            V.w[NW / 2 + i] = even ? t0 : P.w[NW / 2 + i];
+        }
+        if (pool) {
+            A = V;
+#pragma unroll
+            for (int i = 0; i < NW; i++) B.w[i] = 0;
+        } else {
+            quant(A, c, choice);
+            quant(B, c, choice);
+        }
+    } else {
+        quant(A, c, choice);
+        quant(B, c, choice);
+    }
+    const uint32_t wrate = __reduce_max_sync(0xffffffffu, rate);
+#pragma unroll
+    for (uint32_t grp = 0; grp < (uint32_t)NG; grp++) {
+        if (wrate <= 8u * grp) break;
+        uint32_t aL, aH, bL, bH;
+        row_planes(A, grp, aL, aH);
+        row_planes(B, grp, bL, bH);
+        uint32_t y1 = xpose4(aL, r), y2 = xpose4(bL, r), y3 = xpose4(aH, r), y4 = xpose4(bH, r);
+        const uint32_t pl = 8u * grp + r;  // planes pl and pl + 4
+        if (pool) {
+            y1 = __byte_perm(y1, 0, 0x3120);  // row pairs were taken in the order 0,2,1,3
+            y3 = __byte_perm(y3, 0, 0x3120);
+            if (active && pl < rate) *reinterpret_cast<uint32_t *>(dst + 4u * pl) = y1;
+            if (active && pl + 4u < rate) *reinterpret_cast<uint32_t *>(dst + 4u * (pl + 4u)) = y3;
+        } else {
+            // block payloads start at multiples of 4 bytes only (a pooled block
+            // has 4 bytes per plane), so the plane pairs go out as two words
+            if (active && pl < rate) {
+                *reinterpret_cast<uint32_t *>(dst + 8u * pl) = y1;
+                *reinterpret_cast<uint32_t *>(dst + 8u * pl + 4u) = y2;
+            }
+            if (active && pl + 4u < rate) {
+                *reinterpret_cast<uint32_t *>(dst + 8u * (pl + 4u)) = y3;
+                *reinterpret_cast<uint32_t *>(dst + 8u * (pl + 4u) + 4u) = y4;
+            }
+        }
+    }
+}
+
+// Compute warps: per tile, pass A from the input ring into registers and
+// header bytes, tile scan and aggregate publication, pass B into the
+// payload ring.
+template <typename T, int VEC, int BINS, bool POOL>
+__device__ __forceinline__ void enc_compute(const EncArgs<T> &a, EncSmem &sm)
+{
+    constexpr int UMAX = Elem<T>::kTileBlocks / 8 / kEncWarps;  // units per warp per tile
     const Geom &g = a.g;
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t jb = lane & 7, r = lane >> 3;
-
-    if (tid == 0) {
-        for (int s = 0; s < kStages; s++) mbar_init(&sm.bar[s], 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncthreads();
-    if (tid == 0) {
-        for (int s = 0; s < kStages; s++) {
-            unsigned long long t = atomicAdd(&a.ctl->ticket, 1ull);
-            enc_issue<VEC>(a, sm, s, t);
+    uint32_t consumed = 0;  // input-ring entries whose load this loop has waited for
+    for (uint32_t k = 0;; k++) {
+        const int i = (int)(k % kInStages), j = (int)(k % kStStages);
+        const uint32_t n = k / kInStages, m = k / kStStages;
+        bool ok = mbar_wait(&sm.in_full[i], n & 1u, a.ctl);
+        if (!compute_bar_and(ok)) break;
+        consumed = k + 1;
+        const unsigned long long t = sm.in_tile[i];
+        if (t >= g.ntiles) {
+            // end of this CTA's tiles: hand the end marker to the writer
+            if (tid == 0 && mbar_wait(&sm.st_empty[j], (m & 1u) ^ 1u, a.ctl)) {
+                sm.st_tile[j] = t;
+                mbar_arrive(&sm.st_full[j]);
+            }
+            break;
         }
-    }
-
-    uint32_t it = 0;
-    bool clean = false;
-    for (;; it++) {
-        const int s = it & 1;
-        const uint32_t parity = (it >> 1) & 1u;
-        bool ok = mbar_wait(&sm.bar[s], parity, a.ctl);
-        if (!__syncthreads_and(ok)) break;  // every TMA this CTA issued has landed or timed out
-        const unsigned long long t = sm.tile[s];
-        if (t >= g.ntiles) { clean = true; break; }
         const TileInfo ti = tile_info(g, t);
-        const uint8_t *stage = sm.stage[s];
-
-        // block-row table for whole-row tiles
+        const uint8_t *stage = sm.in[i];
         if (!g.chunked) {
             if (tid < ti.nbr) {
-                uint32_t nrows;
+                uint32_t nrows, n0;
                 unsigned long long rs = brow_start(g, ti.rho0 + tid, nrows);
-                uint32_t n0;
                 unsigned long long r0 = brow_start(g, ti.rho0, n0);
                 sm.br_rel[tid] = (uint32_t)((rs - r0) * g.Z);
                 sm.br_rows[tid] = (uint8_t)nrows;
@@ -446,315 +844,368 @@ __global__ void __launch_bounds__(kThreads, 2) enc_kernel(const EncArgs a)
             brow_start(g, ti.rho0, nrows);
             sm.br_rows[0] = (uint8_t)nrows;
         }
-        __syncthreads();
+        compute_bar();
 
+        // ---- pass A: rows to registers, header bytes
         const uint32_t nunits = (ti.nblk + 7) >> 3;
-        // ---- pass A: statistics -> header byte per block
-        for (uint32_t u = warp; u < nunits; u += kWarps) {
-            const uint32_t b = u * 8 + jb;
-            const bool active = b < ti.nblk;
-            uint32_t wA[4] = {0, 0, 0, 0}, wB[4] = {0, 0, 0, 0};
-            SegLoc L = seg_locate<true>(g, ti, sm.br_rel, sm.br_rows, stage, sm.mis[s], active ? b : 0, r);
-            if (active && r < L.nrows) { load8<VEC>(L.pA, wA); if (L.ncols < 8) mask_cols(wA, L.ncols); }
-            if (active && r + 4 < L.nrows) { load8<VEC>(L.pB, wB); if (L.ncols < 8) mask_cols(wB, L.ncols); }
-
-            uint32_t choice = 3;
-            if (BINS == BINS_MONO) {
-                // choice = interval of the smallest value >= bin0 (counts of
-                // cuLSZ_kernel.cu:906-935 are equal exactly when an interval is empty)
-                uint32_t mn = 0xffffffffu;
-                const uint32_t b0 = a.c.binc[0];
+        Row<T> A[UMAX], B[UMAX];
+        uint32_t hq[UMAX];
+        uint32_t bad = 0;
 #pragma unroll
-                for (int i = 0; i < 4; i++) {
-                    mn = min(mn, (wA[i] & 0xffffu) - b0); mn = min(mn, (wA[i] >> 16) - b0);
-                    mn = min(mn, (wB[i] & 0xffffu) - b0); mn = min(mn, (wB[i] >> 16) - b0);
+        for (int q = 0; q < UMAX; q++) {
+            const uint32_t u = warp + (uint32_t)q * kEncWarps;
+            hq[q] = 0;
+            if (u < nunits) {
+                const uint32_t b = u * 8 + jb;
+                const bool active = b < ti.nblk;
+                SegLoc L = seg_locate<T, true>(g, ti, sm.br_rel, sm.br_rows, stage, sm.in_mis[i], active ? b : 0, r);
+                load_rows<T, VEC>(L, active, r, A[q], B[q]);
+                uint32_t rb;
+                hq[q] = block_header<T, BINS, POOL>(A[q], B[q], a.c, rb);
+                if (active && r == 0) {
+                    sm.hdr[b] = (uint8_t)hq[q];
+                    bad |= rb;
                 }
-                mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, 8));
-                mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, 16));
-                const uint32_t v = mn + b0;  // smallest value >= bin0 (if any)
-                const bool any = mn < 0x80000000u;
-                choice = (any && v < a.c.binc[1]) ? 0u : (any && v < a.c.binc[2]) ? 1u : (any && v < a.c.binc[3]) ? 2u : 3u;
-            } else if (BINS == BINS_GENERAL) {
-                uint32_t cnt = 0;  // four 8-bit counters
-#pragma unroll
-                for (int i = 0; i < 8; i++) {
-                    uint32_t w = i < 4 ? wA[i] : wB[i - 4];
-#pragma unroll
-                    for (int h = 0; h < 2; h++) {
-                        uint32_t v = h ? (w >> 16) : (w & 0xffffu);
-                        cnt += (v < a.c.binc[0]) | ((v < a.c.binc[1]) << 8) | ((v < a.c.binc[2]) << 16) |
-                               ((uint32_t)(v < a.c.binc[3]) << 24);
-                    }
-                }
-                cnt += __shfl_xor_sync(0xffffffffu, cnt, 8);
-                cnt += __shfl_xor_sync(0xffffffffu, cnt, 16);
-                uint32_t c0 = cnt & 0xff, c1 = (cnt >> 8) & 0xff, c2 = (cnt >> 16) & 0xff, c3 = cnt >> 24;
-                choice = 0;
-                if (c1 == c0) { choice = 1; if (c2 == c1) { choice = 2; if (c3 == c2) choice = 3; } }
             }
-            bool pool = false;
-            if (POOL) {
-                uint32_t zc = 0;
-#pragma unroll
-                for (int i = 0; i < 4; i++) zc += zero_halves(wA[i]) + zero_halves(wB[i]);
-                zc += __shfl_xor_sync(0xffffffffu, zc, 8);
-                zc += __shfl_xor_sync(0xffffffffu, zc, 16);
-                pool = (int)zc >= a.c.pool_min;
-            }
-            const uint32_t m = a.c.magic[choice];
-            uint32_t orv = 0;
-            if (pool) {
-                uint32_t p0, p1, p2, p3;
-                pool_row(wA, p0, p1);
-                pool_row(wB, p2, p3);
-                orv = quant2(p0, m) | quant2(p1, m) | quant2(p2, m) | quant2(p3, m);
-            } else {
-#pragma unroll
-                for (int i = 0; i < 4; i++) orv |= quant2(wA[i], m) | quant2(wB[i], m);
-            }
-            orv |= __shfl_xor_sync(0xffffffffu, orv, 8);
-            orv |= __shfl_xor_sync(0xffffffffu, orv, 16);
-            const uint32_t rate = bitlen((orv & 0xffffu) | (orv >> 16));
-            if (active && r == 0) sm.hdr[b] = (uint8_t)((pool ? 0x80u : 0u) | (choice << 5) | rate);
         }
-        __syncthreads();
+        if (bad) sm.range_err = 1;
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&sm.in_empty[i]);  // the input slot may be refilled
+        compute_bar();
+        if (sm.range_err) {
+            // a uint32 quotient >= 2^31 needs 32 planes, which the 5-bit rate
+            // field cannot hold
+            if (tid == 0) raise_error(a.ctl, DEV_ERR_RANGE);
+            break;
+        }
 
-        // ---- tile size, look-back, stream offset
+        // ---- tile scan; the aggregate goes out before anything waits on the writer
         if (warp == 0) {
-            uint32_t agg = tile_scan(sm.hdr, sm.off, ti.nblk);
-            bool lok;
-            unsigned long long excl = tile_prefix(a.state, t, a.epoch, agg, a.ctl, lok);
+            const uint32_t agg = tile_scan(sm.hdr, sm.off, ti.nblk);
             if (lane == 0) {
-                sm.base = excl;
                 sm.agg = agg;
-                sm.flag_ok = lok ? 1u : 0u;
-                if (lok && g.R + excl + agg > a.cap) {
-                    raise_error(a.ctl, DEV_ERR_CAPACITY);
-                    sm.flag_ok = 0;
-                }
-                if (lok && t == g.ntiles - 1 && sm.flag_ok) {
-                    a.ctl->total = excl + agg;
-                    a.ctl->stream_len = g.R + excl + agg;
-                    if (a.sizes_out) {
-                        a.sizes_out[0] = g.R + excl + agg;
-                        a.sizes_out[1] = excl + agg;
-                    }
-                }
+                st_release_u64(a.state + t, make_state(a.epoch, t == 0 ? kFlagIncl : kFlagAgg, agg));
             }
         }
-        __syncthreads();
-        if (!sm.flag_ok) break;
+        for (uint32_t b = tid; b < ti.nblk; b += kEncWarps * 32) a.out[ti.k0 + b] = sm.hdr[b];
+        bool free_ok = true;
+        if (tid == 0) free_ok = mbar_wait(&sm.st_empty[j], (m & 1u) ^ 1u, a.ctl);
+        if (!compute_bar_and(free_ok)) break;
 
-        // ---- headers of this tile (and the zero pad after the last header)
-        for (uint32_t b = tid; b < ti.nblk; b += kThreads) a.out[ti.k0 + b] = sm.hdr[b];
-        if (t == g.ntiles - 1 && tid < (uint32_t)(g.R - g.nb)) a.out[g.nb + tid] = 0;
-
-        // ---- pass B: pack bit planes into the stream
-        uint8_t *const pay = a.out + g.R + sm.base;
-        for (uint32_t u = warp; u < nunits; u += kWarps) {
-            const uint32_t b = u * 8 + jb;
-            const bool active = b < ti.nblk;
-            uint32_t wA[4] = {0, 0, 0, 0}, wB[4] = {0, 0, 0, 0};
-            SegLoc L = seg_locate<true>(g, ti, sm.br_rel, sm.br_rows, stage, sm.mis[s], active ? b : 0, r);
-            if (active && r < L.nrows) { load8<VEC>(L.pA, wA); if (L.ncols < 8) mask_cols(wA, L.ncols); }
-            if (active && r + 4 < L.nrows) { load8<VEC>(L.pB, wB); if (L.ncols < 8) mask_cols(wB, L.ncols); }
-            const uint32_t h = active ? sm.hdr[b] : 0u;
-            const bool pool = (h & 0x80u) != 0;
-            const uint32_t rate = h & 0x1fu;
-            const uint32_t m = a.c.magic[(h >> 5) & 3u];
-            // the 8 values this lane transposes ("virtual row"): plain blocks
-            // use rows r and r+4 as they are
-            uint32_t v0 = quant2(wA[0], m), v1 = quant2(wA[1], m), v2 = quant2(wA[2], m), v3 = quant2(wA[3], m);
-            uint32_t u0 = quant2(wB[0], m), u1 = quant2(wB[1], m), u2 = quant2(wB[2], m), u3 = quant2(wB[3], m);
-            if (__any_sync(0xffffffffu, active && pool)) {
-                // pooled blocks: lane r=0 takes rows 0,1; r=1 rows 4,5; r=2 rows 2,3;
-                // r=3 rows 6,7 (one pooled byte row pair each)
-                uint32_t p0, p1, p2, p3;
-                pool_row(wA, p0, p1);
-                pool_row(wB, p2, p3);
-                p0 = quant2(p0, m); p1 = quant2(p1, m); p2 = quant2(p2, m); p3 = quant2(p3, m);
-                const bool even = (r & 1u) == 0;
-                const uint32_t t0 = __shfl_xor_sync(0xffffffffu, even ? p2 : p0, 8);
-                const uint32_t t1 = __shfl_xor_sync(0xffffffffu, even ? p3 : p1, 8);
-                if (pool) {
-                    v0 = even ? p0 : t0; v1 = even ? p1 : t1;
-                    v2 = even ? t0 : p2; v3 = even ? t1 : p3;
-                    u0 = u1 = u2 = u3 = 0;
-                }
-            }
-            const uint32_t wrate = __reduce_max_sync(0xffffffffu, rate);
-            uint8_t *const dst = pay + (active ? sm.off[b] : 0u);
-            for (uint32_t hi = 0; hi < 2; hi++) {
-                if (wrate <= 8u * hi) break;
-                uint32_t aL, aH, bL = 0, bH = 0;
-                lsc_row_planes(v0, v1, v2, v3, (int)hi, aL, aH);
-                lsc_row_planes(u0, u1, u2, u3, (int)hi, bL, bH);
-                uint32_t y1 = xpose4(aL, r), y2 = xpose4(bL, r), y3 = xpose4(aH, r), y4 = xpose4(bH, r);
-                const uint32_t pl = 8u * hi + r;  // planes pl and pl + 4
-                if (pool) {
-                    y1 = __byte_perm(y1, 0, 0x3120);
-                    y3 = __byte_perm(y3, 0, 0x3120);
-                    if (active && pl < rate) *reinterpret_cast<uint32_t *>(dst + 4u * pl) = y1;
-                    if (active && pl + 4u < rate) *reinterpret_cast<uint32_t *>(dst + 4u * (pl + 4u)) = y3;
-                } else {
-                    if (active && pl < rate) {
-                        *reinterpret_cast<uint32_t *>(dst + 8u * pl) = y1;
-                        *reinterpret_cast<uint32_t *>(dst + 8u * pl + 4u) = y2;
-                    }
-                    if (active && pl + 4u < rate) {
-                        *reinterpret_cast<uint32_t *>(dst + 8u * (pl + 4u)) = y3;
-                        *reinterpret_cast<uint32_t *>(dst + 8u * (pl + 4u) + 4u) = y4;
-                    }
-                }
+        // ---- pass B: pack from registers into the payload ring
+        uint8_t *const st = sm.st[j];
+#pragma unroll
+        for (int q = 0; q < UMAX; q++) {
+            const uint32_t u = warp + (uint32_t)q * kEncWarps;
+            if (u < nunits) {
+                const uint32_t b = u * 8 + jb;
+                const bool active = b < ti.nblk;
+                block_pack<T>(A[q], B[q], hq[q], active, r, a.c, st + (active ? sm.off[b] : 0u));
             }
         }
-        __syncthreads();  // stage s fully consumed
+        compute_bar();
         if (tid == 0) {
-            unsigned long long nt = aborted(a.ctl) ? g.ntiles : atomicAdd(&a.ctl->ticket, 1ull);
-            enc_issue<VEC>(a, sm, s, nt);
+            sm.st_tile[j] = t;
+            sm.st_agg[j] = sm.agg;
+            mbar_arrive(&sm.st_full[j]);
         }
     }
-    // Leaving early (error): the copy issued into the other stage must land
-    // before the CTA's shared memory is released.  Bounded like every wait.
-    if (!clean && tid == 0) {
-        const int o = (it + 1) & 1;
-        mbar_wait(&sm.bar[o], ((it + 1) >> 1) & 1u, a.ctl);
+    if (tid == 0) sm.consumed = consumed;
+}
+
+// Producer warp: claims tiles in ticket order and fills the input ring.
+template <typename T>
+__device__ __forceinline__ void enc_producer(const EncArgs<T> &a, EncSmem &sm)
+{
+    const uint32_t lane = threadIdx.x & 31;
+    uint32_t k = 0;
+    for (;; k++) {
+        const int i = (int)(k % kInStages);
+        const uint32_t n = k / kInStages;
+        bool ok = mbar_wait(&sm.in_empty[i], (n & 1u) ^ 1u, a.ctl);
+        if (!__all_sync(0xffffffffu, ok)) break;
+        unsigned long long t = 0;
+        if (lane == 0) {
+            t = aborted(a.ctl) ? a.g.ntiles : atomicAdd(&a.ctl->ticket, 1ull);
+            enc_issue<T>(a, sm, i, t);
+        }
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= a.g.ntiles) {
+            k++;
+            break;
+        }
+    }
+    if (lane == 0) sm.issued = k;
+}
+
+// Writer warp: for each packed tile, the decoupled look-back for its stream
+// offset, publication of the inclusive prefix, and the copy of the payload
+// from the ring to the stream.
+template <typename T>
+__device__ __forceinline__ void enc_writer(const EncArgs<T> &a, EncSmem &sm)
+{
+    const Geom &g = a.g;
+    const uint32_t lane = threadIdx.x & 31;
+    for (uint32_t k = 0;; k++) {
+        const int j = (int)(k % kStStages);
+        const uint32_t m = k / kStStages;
+        bool ok = mbar_wait(&sm.st_full[j], m & 1u, a.ctl);
+        if (!__all_sync(0xffffffffu, ok)) break;
+        const unsigned long long t = sm.st_tile[j];
+        if (t >= g.ntiles) break;
+        const uint32_t agg = sm.st_agg[j];
+        unsigned long long excl = 0;
+        bool lok = true;
+        if (t > 0) {
+            excl = lookback_warp(a.state, t, a.epoch, a.ctl, lok);
+            if (!lok) break;
+            if (lane == 0) st_release_u64(a.state + t, make_state(a.epoch, kFlagIncl, excl + agg));
+        }
+        if (g.R + excl + agg > a.cap) {
+            if (lane == 0) raise_error(a.ctl, DEV_ERR_CAPACITY);
+            break;
+        }
+        // copy [0, agg) of the ring slot to out + R + excl (4-byte aligned):
+        // 4-byte words up to the first 16-byte boundary, 16-byte stores after
+        const uint8_t *src = sm.st[j];
+        uint8_t *dst = a.out + g.R + excl;
+        uint32_t head = (uint32_t)((16u - ((uintptr_t)dst & 15u)) & 15u);
+        if (head > agg) head = agg;
+        if (lane < head / 4u) reinterpret_cast<uint32_t *>(dst)[lane] = reinterpret_cast<const uint32_t *>(src)[lane];
+        const uint32_t nbody = (agg - head) / 16u;
+        for (uint32_t c = lane; c < nbody; c += 32) {
+            const uint32_t *s4 = reinterpret_cast<const uint32_t *>(src + head + 16u * c);
+            *reinterpret_cast<uint4 *>(dst + head + 16u * c) = make_uint4(s4[0], s4[1], s4[2], s4[3]);
+        }
+        const uint32_t tail = head + 16u * nbody;
+        if (lane < (agg - tail) / 4u)
+            reinterpret_cast<uint32_t *>(dst + tail)[lane] = reinterpret_cast<const uint32_t *>(src + tail)[lane];
+        if (t == g.ntiles - 1) {
+            if (lane == 0) {
+                a.ctl->total = excl + agg;
+                a.ctl->stream_len = g.R + excl + agg;
+                if (a.sizes_out) {
+                    a.sizes_out[0] = g.R + excl + agg;
+                    a.sizes_out[1] = excl + agg;
+                }
+            }
+            if (lane < (uint32_t)(g.R - g.nb)) a.out[g.nb + lane] = 0;  // header pad
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&sm.st_empty[j]);
+    }
+}
+
+template <typename T, int VEC, int BINS, bool POOL>
+__global__ void __launch_bounds__(kEncThreads, 1) enc_kernel(const EncArgs<T> a)
+{
+    extern __shared__ __align__(128) uint8_t smem_raw[];
+    EncSmem &sm = *reinterpret_cast<EncSmem *>(smem_raw);
+    const uint32_t tid = threadIdx.x, warp = tid >> 5;
+    if (tid == 0) {
+        for (int s = 0; s < kInStages; s++) {
+            mbar_init(&sm.in_full[s], 1);
+            mbar_init(&sm.in_empty[s], kEncWarps);
+        }
+        for (int s = 0; s < kStStages; s++) {
+            mbar_init(&sm.st_full[s], 1);
+            mbar_init(&sm.st_empty[s], 1);
+        }
+        sm.range_err = 0;
+        sm.consumed = 0;
+        sm.issued = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
+    if (warp < (uint32_t)kEncWarps)
+        enc_compute<T, VEC, BINS, POOL>(a, sm);
+    else if (warp == (uint32_t)kProducerWarp)
+        enc_producer<T>(a, sm);
+    else
+        enc_writer<T>(a, sm);
+    __syncthreads();
+    // After an error a load may still be in flight into a slot nobody
+    // consumed; it must land before the CTA's shared memory is released.
+    if (tid == (uint32_t)kProducerWarp * 32) {
+        for (uint32_t u = sm.consumed; u < sm.issued; u++)
+            mbar_wait(&sm.in_full[u % kInStages], (u / kInStages) & 1u, a.ctl);
+    }
 }
 
 // ---------------------------------------------------------------- decoder
-template <int VEC>
-__global__ void __launch_bounds__(kThreads, 4) dec_kernel(const DecArgs a)
+// Decoding needs no look-back on the critical path: the header bytes hold
+// every block's size, so a small first kernel turns them into per-tile
+// stream offsets and the decode kernel then runs every tile independently.
+constexpr int kSegTiles = 32;  // tiles per segment of the offsets kernel (one per lane of warp 0)
+
+// Per-tile payload offsets (relative to roundup4(nb)) from the header bytes
+// (sizes as in lsCOMP/src/cuLSZ_kernel.cu:1333-1339), tile_off[t].  Segments
+// of kSegTiles tiles are claimed in order and chained by the look-back.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) dec_offsets_kernel(const DecArgs<T> a)
 {
+    __shared__ unsigned long long seg_s;
+    __shared__ uint32_t tsum[kSegTiles];
+    __shared__ uint32_t ok_s;
+    const Geom &g = a.g;
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const unsigned long long nseg = (g.ntiles + kSegTiles - 1) / kSegTiles;
+    for (;;) {
+        if (tid == 0) seg_s = aborted(a.ctl) ? nseg : atomicAdd(&a.ctl->ticket, 1ull);
+        __syncthreads();
+        const unsigned long long sg = seg_s;
+        if (sg >= nseg) break;
+        const unsigned long long t0 = sg * kSegTiles;
+        for (uint32_t q = warp; q < (uint32_t)kSegTiles; q += kWarps) {
+            const unsigned long long t = t0 + q;
+            uint32_t sum = 0;
+            if (t < g.ntiles) {
+                const TileInfo ti = tile_info(g, t);
+                for (uint32_t b = lane; b < ti.nblk; b += 32) {
+                    const uint32_t h = a.in[ti.k0 + b];
+                    sum += (h & 0x1fu) * ((h & 0x80u) ? 4u : 8u);
+                }
+            }
+            sum = __reduce_add_sync(0xffffffffu, sum);
+            if (lane == 0) tsum[q] = sum;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            const uint32_t v = tsum[lane];
+            uint32_t inc = v;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t x = __shfl_up_sync(0xffffffffu, inc, o);
+                if (lane >= (uint32_t)o) inc += x;
+            }
+            const uint32_t agg = __shfl_sync(0xffffffffu, inc, 31);
+            bool lok;
+            const unsigned long long base = tile_prefix(a.state, sg, a.epoch, agg, a.ctl, lok);
+            if (lok && t0 + lane < g.ntiles) a.tile_off[t0 + lane] = base + (inc - v);
+            if (lane == 0) ok_s = lok ? 1u : 0u;
+        }
+        __syncthreads();
+        if (!ok_s) break;
+    }
+}
+
+// One CTA per tile: header bytes -> in-tile offsets -> plane words of each
+// block -> values scattered to the output rows
+// (lsCOMP/src/cuLSZ_kernel.cu:1440-1640).  Every element of the tile is
+// written, zeros for blocks of rate 0.
+template <typename T, int VEC>
+__global__ void __launch_bounds__(kThreads, 4) dec_kernel(const DecArgs<T> a)
+{
+    constexpr int NW = Elem<T>::kWords;
+    constexpr int NG = Elem<T>::kGroups;
     __shared__ DecSmem sm;
     const Geom &g = a.g;
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t jb = lane & 7, r = lane >> 3;
+    const bool even = (r & 1u) == 0;
+    const unsigned long long t = blockIdx.x;
+    if (t >= g.ntiles) return;
 
-    for (;;) {
-        if (tid == 0) sm.tile = aborted(a.ctl) ? g.ntiles : atomicAdd(&a.ctl->ticket, 1ull);
-        __syncthreads();
-        const unsigned long long t = sm.tile;
-        if (t >= g.ntiles) break;
-        const TileInfo ti = tile_info(g, t);
-        unsigned long long row0 = 0;
-        {
-            uint32_t n0;
-            row0 = brow_start(g, ti.rho0, n0);
-        }
-        if (!g.chunked) {
-            if (tid < ti.nbr) {
-                uint32_t nrows;
-                unsigned long long rs = brow_start(g, ti.rho0 + tid, nrows);
-                sm.br_rel[tid] = (uint32_t)((rs - row0) * g.Z);
-                sm.br_rows[tid] = (uint8_t)nrows;
-            }
-        } else if (tid == 0) {
+    const TileInfo ti = tile_info(g, t);
+    uint32_t n0;
+    const unsigned long long row0 = brow_start(g, ti.rho0, n0);
+    if (!g.chunked) {
+        if (tid < ti.nbr) {
             uint32_t nrows;
-            brow_start(g, ti.rho0, nrows);
-            sm.br_rows[0] = (uint8_t)nrows;
+            unsigned long long rs = brow_start(g, ti.rho0 + tid, nrows);
+            sm.br_rel[tid] = (uint32_t)((rs - row0) * g.Z);
+            sm.br_rows[tid] = (uint8_t)nrows;
         }
-        for (uint32_t b = tid; b < ti.nblk; b += kThreads) sm.hdr[b] = a.in[ti.k0 + b];
-        __syncthreads();
-        if (warp == 0) {
-            uint32_t agg = tile_scan(sm.hdr, sm.off, ti.nblk);
-            bool lok;
-            unsigned long long excl = tile_prefix(a.state, t, a.epoch, agg, a.ctl, lok);
-            if (lane == 0) {
-                sm.base = excl;
-                sm.agg = agg;
-                sm.flag_ok = lok ? 1u : 0u;
-                if (lok && g.R + excl + agg > a.cap) {
-                    raise_error(a.ctl, DEV_ERR_CAPACITY);
-                    sm.flag_ok = 0;
-                }
+    } else if (tid == 0) {
+        sm.br_rows[0] = (uint8_t)n0;
+    }
+    for (uint32_t b = tid; b < ti.nblk; b += kThreads) sm.hdr[b] = a.in[ti.k0 + b];
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t agg = tile_scan(sm.hdr, sm.off, ti.nblk);
+        if (lane == 0) {
+            const unsigned long long base = a.tile_off[t];
+            sm.base = base;
+            sm.flag_ok = 1u;
+            if (g.R + base + agg > a.cap) {
+                raise_error(a.ctl, DEV_ERR_CAPACITY);
+                sm.flag_ok = 0;
             }
         }
-        __syncthreads();
-        if (!sm.flag_ok) break;
+    }
+    __syncthreads();
+    if (!sm.flag_ok) return;
 
-        const uint8_t *const pay = a.in + g.R + sm.base;
-        const unsigned long long ebase = row0 * g.Z;  // element index of the tile's first row
-        const uint32_t nunits = (ti.nblk + 7) >> 3;
-        for (uint32_t u = warp; u < nunits; u += kWarps) {
-            const uint32_t b = u * 8 + jb;
-            const bool active = b < ti.nblk;
-            SegLoc L = seg_locate<false>(g, ti, sm.br_rel, sm.br_rows, nullptr, nullptr, active ? b : 0, r);
-            const uint32_t h = active ? sm.hdr[b] : 0u;
-            const bool pool = (h & 0x80u) != 0;
-            const uint32_t rate = h & 0x1fu;
-            const uint32_t bin = a.c.bins[(h >> 5) & 3u];
-            const uint8_t *src = pay + (active ? sm.off[b] : 0u);
-            const uint32_t wrate = __reduce_max_sync(0xffffffffu, rate);
-            uint32_t pl_[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};  // [hi][aL, bL, aH, bH] after transpose back
-            for (uint32_t hi = 0; hi < 2; hi++) {
-                if (wrate <= 8u * hi) break;
-                const uint32_t pl = 8u * hi + r;
-                uint32_t y1 = 0, y2 = 0, y3 = 0, y4 = 0;
-                if (pool) {
-                    if (pl < rate) y1 = *reinterpret_cast<const uint32_t *>(src + 4u * pl);
-                    if (pl + 4u < rate) y3 = *reinterpret_cast<const uint32_t *>(src + 4u * (pl + 4u));
-                    y1 = __byte_perm(y1, 0, 0x3120);
-                    y3 = __byte_perm(y3, 0, 0x3120);
-                } else {
-                    if (pl < rate) {
-                        y1 = *reinterpret_cast<const uint32_t *>(src + 8u * pl);
-                        y2 = *reinterpret_cast<const uint32_t *>(src + 8u * pl + 4u);
-                    }
-                    if (pl + 4u < rate) {
-                        y3 = *reinterpret_cast<const uint32_t *>(src + 8u * (pl + 4u));
-                        y4 = *reinterpret_cast<const uint32_t *>(src + 8u * (pl + 4u) + 4u);
-                    }
-                }
-                pl_[hi][0] = xpose4(y1, r);
-                pl_[hi][1] = xpose4(y2, r);
-                pl_[hi][2] = xpose4(y3, r);
-                pl_[hi][3] = xpose4(y4, r);
-            }
-            // rebuild the quantised values of this lane's virtual row(s)
-            uint32_t wA[4], wB[4];
-            lsc_row_values(pl_[0][0], pl_[0][2], pl_[1][0], pl_[1][2], wA[0], wA[1], wA[2], wA[3]);
-            lsc_row_values(pl_[0][1], pl_[0][3], pl_[1][1], pl_[1][3], wB[0], wB[1], wB[2], wB[3]);
-            if (__any_sync(0xffffffffu, active && pool)) {
-                // wA of a pooled lane holds the 8 pooled values of its row pair:
-                // 4 of the first row, then 4 of the second.  Even lanes keep the
-                // first row and send the second; odd lanes the reverse.
-                const bool even = (r & 1u) == 0;
-                const uint32_t t0 = __shfl_xor_sync(0xffffffffu, even ? wA[2] : wA[0], 8);
-                const uint32_t t1 = __shfl_xor_sync(0xffffffffu, even ? wA[3] : wA[1], 8);
-                if (pool) {
-                    uint32_t q[4];
-                    q[0] = even ? wA[0] : t0; q[1] = even ? wA[1] : t1;  // row r
-                    q[2] = even ? t0 : wA[2]; q[3] = even ? t1 : wA[3];  // row r+4
-                    uint32_t e[8];
+    const uint8_t *const pay = a.in + g.R + sm.base;
+    const unsigned long long ebase = row0 * g.Z;  // element index of the tile's first row
+    const uint32_t nunits = (ti.nblk + 7) >> 3;
+    for (uint32_t u = warp; u < nunits; u += kWarps) {
+        const uint32_t b = u * 8 + jb;
+        const bool active = b < ti.nblk;
+        SegLoc L = seg_locate<T, false>(g, ti, sm.br_rel, sm.br_rows, nullptr, nullptr, active ? b : 0, r);
+        const uint32_t h = active ? sm.hdr[b] : 0u;
+        const bool pool = (h & 0x80u) != 0;
+        const uint32_t rate = h & 0x1fu;
+        const uint32_t bin = a.c.bins[(h >> 5) & 3u];
+        const uint8_t *src = pay + (active ? sm.off[b] : 0u);
+        const uint32_t wrate = __reduce_max_sync(0xffffffffu, rate);
+        // plane bytes per byte group, back in row order: [grp][0/1] = lo/hi
+        // half of row r (PA) and of row r+4 (PB)
+        uint32_t PA[NG][2], PB[NG][2];
 #pragma unroll
-                    for (int i = 0; i < 4; i++) {
-                        // de-quantise and repeat each pooled value over its two columns
-                        uint32_t lo = (q[i] & 0xffffu) * bin, hi = (q[i] >> 16) * bin;
-                        e[2 * i] = (lo & 0xffffu) | (lo << 16);
-                        e[2 * i + 1] = (hi & 0xffffu) | (hi << 16);
-                    }
-                    wA[0] = e[0]; wA[1] = e[1]; wA[2] = e[2]; wA[3] = e[3];
-                    wB[0] = e[4]; wB[1] = e[5]; wB[2] = e[6]; wB[3] = e[7];
+        for (uint32_t grp = 0; grp < (uint32_t)NG; grp++) {
+            PA[grp][0] = PA[grp][1] = PB[grp][0] = PB[grp][1] = 0;
+            if (wrate <= 8u * grp) continue;
+            const uint32_t pl = 8u * grp + r;
+            uint32_t y1 = 0, y2 = 0, y3 = 0, y4 = 0;
+            if (pool) {
+                if (pl < rate) y1 = *reinterpret_cast<const uint32_t *>(src + 4u * pl);
+                if (pl + 4u < rate) y3 = *reinterpret_cast<const uint32_t *>(src + 4u * (pl + 4u));
+                y1 = __byte_perm(y1, 0, 0x3120);
+                y3 = __byte_perm(y3, 0, 0x3120);
+            } else {
+                if (pl < rate) {
+                    y1 = *reinterpret_cast<const uint32_t *>(src + 8u * pl);
+                    y2 = *reinterpret_cast<const uint32_t *>(src + 8u * pl + 4u);
+                }
+                if (pl + 4u < rate) {
+                    y3 = *reinterpret_cast<const uint32_t *>(src + 8u * (pl + 4u));
+                    y4 = *reinterpret_cast<const uint32_t *>(src + 8u * (pl + 4u) + 4u);
                 }
             }
-            if (!pool && bin != 1u) {
+            PA[grp][0] = xpose4(y1, r);
+            PB[grp][0] = xpose4(y2, r);
+            PA[grp][1] = xpose4(y3, r);
+            PB[grp][1] = xpose4(y4, r);
+        }
+        Row<T> A, B;
+        row_values(PA, A);
+        row_values(PB, B);
+        if (__any_sync(0xffffffffu, active && pool)) {
+            // a pooled lane holds the 8 pooled values of its row pair: 4 of
+            // the first row, then 4 of the second.  Even lanes keep the
+            // first row and send the second; odd lanes the reverse.
+            Row<T> Q;
 #pragma unroll
-                for (int i = 0; i < 4; i++) {
-                    uint32_t lo = (wA[i] & 0xffffu) * bin, hi = (wA[i] >> 16) * bin;
-                    wA[i] = (lo & 0xffffu) | (hi << 16);
-                    lo = (wB[i] & 0xffffu) * bin; hi = (wB[i] >> 16) * bin;
-                    wB[i] = (lo & 0xffffu) | (hi << 16);
-                }
+            for (int i = 0; i < NW / 2; i++) {
+                const uint32_t t0 = __shfl_xor_sync(0xffffffffu, even ? A.w[NW / 2 + i] : A.w[i], 8);
+                Q.w[i] = even ? A.w[i] : t0;                    // row r
+                Q.w[NW / 2 + i] = even ? t0 : A.w[NW / 2 + i];  // row r+4
             }
-            if (active) {
-                uint16_t *rowA = a.out + ebase + L.growA;
-                if (r < L.nrows) store8<VEC>(rowA, wA, L.ncols);
-                if (r + 4 < L.nrows) store8<VEC>(rowA + 4ull * g.Z, wB, L.ncols);
+            if (pool) {
+                A = unpool_row(Q, false, bin);
+                B = unpool_row(Q, true, bin);
             }
         }
-        __syncthreads();
+        if (!pool) {
+            dequant(A, bin);
+            dequant(B, bin);
+        }
+        if (active) {
+            T *rowA = a.out + ebase + L.growA;
+            if (r < L.nrows) store8<VEC>(rowA, A, L.ncols);
+            if (r + 4 < L.nrows) store8<VEC>(rowA + 4ull * g.Z, B, L.ncols);
+        }
     }
 }
 

@@ -74,3 +74,30 @@ void cuLSZ_decompression_uint16_bsize64(uint16_t *d_decData, unsigned char *d_cm
     check(lscomp_decompress_u16(ws, d_cmpBytes, cap, dims.x, dims.y, dims.z, bins, poolingTH, d_decData, stream),
           "cuLSZ_decompression_uint16_bsize64");
 }
+
+// lsCOMP/src/cuLSZ_entry.cu:18-56.  *cmpSize = 32-bit payload total + nb, as
+// the reference computes it.
+void cuLSZ_compression_uint32_bsize64(uint32_t *d_oriData, unsigned char *d_cmpBytes, size_t *cmpSize, uint3 dims,
+                                      uint4 quantBins, float poolingTH, cudaStream_t stream)
+{
+    const uint32_t bins[4] = {quantBins.x, quantBins.y, quantBins.z, quantBins.w};
+    lscomp_workspace *ws = workspace_for(stream);
+    uint64_t cap = lscomp_max_stream_bytes_u32(dims.x, dims.y, dims.z);
+    uint64_t stream_len = 0, ref_size = 0;
+    check(lscomp_compress_u32(ws, d_oriData, dims.x, dims.y, dims.z, bins, poolingTH, d_cmpBytes, cap, &stream_len,
+                              &ref_size, stream),
+          "cuLSZ_compression_uint32_bsize64");
+    if (cmpSize) *cmpSize = (size_t)ref_size;
+}
+
+// lsCOMP/src/cuLSZ_entry.cu:58-91
+void cuLSZ_decompression_uint32_bsize64(uint32_t *d_decData, unsigned char *d_cmpBytes, size_t cmpSize, uint3 dims,
+                                        uint4 quantBins, float poolingTH, cudaStream_t stream)
+{
+    (void)cmpSize;
+    const uint32_t bins[4] = {quantBins.x, quantBins.y, quantBins.z, quantBins.w};
+    lscomp_workspace *ws = workspace_for(stream);
+    uint64_t cap = lscomp_max_stream_bytes_u32(dims.x, dims.y, dims.z);
+    check(lscomp_decompress_u32(ws, d_cmpBytes, cap, dims.x, dims.y, dims.z, bins, poolingTH, d_decData, stream),
+          "cuLSZ_decompression_uint32_bsize64");
+}

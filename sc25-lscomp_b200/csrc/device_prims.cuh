@@ -88,15 +88,20 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
 }
 
 // Bounded wait for the phase with the given parity to complete.  Returns
-// false (after recording DEV_ERR_TIMEOUT) if it does not complete in time.
+// false if another CTA aborted the launch, or (after recording
+// DEV_ERR_TIMEOUT) if the phase does not complete in time.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, LaunchCtl *ctl)
 {
     if (mbar_try_wait(bar, parity)) return true;
-    unsigned long long t0 = global_ns();
+    const unsigned long long t0 = global_ns();
+    uint32_t spins = 0;
     while (!mbar_try_wait(bar, parity)) {
-        if (global_ns() - t0 > kWaitLimitNs) {
-            raise_error(ctl, DEV_ERR_TIMEOUT);
-            return false;
+        if ((++spins & 31u) == 0) {
+            if (aborted(ctl)) return false;
+            if (global_ns() - t0 > kWaitLimitNs) {
+                raise_error(ctl, DEV_ERR_TIMEOUT);
+                return false;
+            }
         }
     }
     return true;

@@ -79,6 +79,12 @@ def load_library() -> ctypes.CDLL:
     lib.lscomp_compress_u16_async.argtypes = [vp, vp, u32, u32, u32, bins_t, f32, vp, u64, vp, vp]
     lib.lscomp_decompress_u16.argtypes = [vp, vp, u64, u32, u32, u32, bins_t, f32, vp, vp]
     lib.lscomp_decompress_u16_async.argtypes = [vp, vp, u64, u32, u32, u32, bins_t, f32, vp, vp]
+    lib.lscomp_max_stream_bytes_u32.restype = u64
+    lib.lscomp_max_stream_bytes_u32.argtypes = [u32, u32, u32]
+    lib.lscomp_compress_u32.argtypes = [vp, vp, u32, u32, u32, bins_t, f32, vp, u64, pu64, pu64, vp]
+    lib.lscomp_compress_u32_async.argtypes = [vp, vp, u32, u32, u32, bins_t, f32, vp, u64, vp, vp]
+    lib.lscomp_decompress_u32.argtypes = [vp, vp, u64, u32, u32, u32, bins_t, f32, vp, vp]
+    lib.lscomp_decompress_u32_async.argtypes = [vp, vp, u64, u32, u32, u32, bins_t, f32, vp, vp]
     _lib = lib
     return lib
 
@@ -100,9 +106,9 @@ def block_count(dims: Sequence[int]) -> int:
     return x * ((y + 7) // 8) * ((z + 7) // 8)
 
 
-def max_stream_bytes(dims: Sequence[int]) -> int:
+def max_stream_bytes(dims: Sequence[int], elem_bytes: int = 2) -> int:
     nb = block_count(dims)
-    return (nb + 3) // 4 * 4 + 128 * nb
+    return (nb + 3) // 4 * 4 + (128 if elem_bytes == 2 else 248) * nb
 
 
 def launch_count() -> int:
@@ -146,19 +152,24 @@ def _stream_handle(stream) -> int:
     return stream.cuda_stream
 
 
+def _suffix(t) -> str:
+    return "u32" if t.element_size() == 4 else "u16"
+
+
 def compress_into(ws: Workspace, d_in, dims, bins, pooling: float, d_out, stream=None) -> Tuple[int, int]:
-    """Compress device tensor d_in (X*Y*Z uint16 in int16) into d_out (uint8).
+    """Compress device tensor d_in (X*Y*Z values: uint16 carried in int16, or
+    uint32 carried in int32) into d_out (uint8).
 
     Returns (stream_len, ref_size): the stream's length in bytes and the size
     the reference's host API reports (payload + nb)."""
     lib = load_library()
     x, y, z = (int(v) for v in dims)
     sl, rs = ctypes.c_uint64(0), ctypes.c_uint64(0)
-    st = lib.lscomp_compress_u16(
+    st = getattr(lib, f"lscomp_compress_{_suffix(d_in)}")(
         ws.handle, ctypes.c_void_p(d_in.data_ptr()), x, y, z, _bins(bins), ctypes.c_float(pooling),
         ctypes.c_void_p(d_out.data_ptr()), ctypes.c_uint64(d_out.numel() * d_out.element_size()),
         ctypes.byref(sl), ctypes.byref(rs), ctypes.c_void_p(_stream_handle(stream)))
-    _check(st, "lscomp_compress_u16")
+    _check(st, f"lscomp_compress_{_suffix(d_in)}")
     return int(sl.value), int(rs.value)
 
 
@@ -167,32 +178,32 @@ def compress_async(ws: Workspace, d_in, dims, bins, pooling: float, d_out, d_siz
     in an int64 tensor) receives {stream_len, payload bytes}."""
     lib = load_library()
     x, y, z = (int(v) for v in dims)
-    st = lib.lscomp_compress_u16_async(
+    st = getattr(lib, f"lscomp_compress_{_suffix(d_in)}_async")(
         ws.handle, ctypes.c_void_p(d_in.data_ptr()), x, y, z, _bins(bins), ctypes.c_float(pooling),
         ctypes.c_void_p(d_out.data_ptr()), ctypes.c_uint64(d_out.numel() * d_out.element_size()),
         ctypes.c_void_p(d_sizes.data_ptr() if d_sizes is not None else 0),
         ctypes.c_void_p(_stream_handle(stream)))
-    _check(st, "lscomp_compress_u16_async")
+    _check(st, f"lscomp_compress_{_suffix(d_in)}_async")
 
 
 def decompress_into(ws: Workspace, d_cmp, cmp_len: int, dims, bins, pooling: float, d_out, stream=None):
     """Decompress the stream in device tensor d_cmp (cmp_len readable bytes)
-    into d_out (X*Y*Z uint16 in int16)."""
+    into d_out (X*Y*Z values, int16 for uint16 data or int32 for uint32)."""
     lib = load_library()
     x, y, z = (int(v) for v in dims)
-    st = lib.lscomp_decompress_u16(
+    st = getattr(lib, f"lscomp_decompress_{_suffix(d_out)}")(
         ws.handle, ctypes.c_void_p(d_cmp.data_ptr()), ctypes.c_uint64(int(cmp_len)), x, y, z, _bins(bins),
         ctypes.c_float(pooling), ctypes.c_void_p(d_out.data_ptr()), ctypes.c_void_p(_stream_handle(stream)))
-    _check(st, "lscomp_decompress_u16")
+    _check(st, f"lscomp_decompress_{_suffix(d_out)}")
 
 
 def decompress_async(ws: Workspace, d_cmp, cmp_len: int, dims, bins, pooling: float, d_out, stream=None):
     lib = load_library()
     x, y, z = (int(v) for v in dims)
-    st = lib.lscomp_decompress_u16_async(
+    st = getattr(lib, f"lscomp_decompress_{_suffix(d_out)}_async")(
         ws.handle, ctypes.c_void_p(d_cmp.data_ptr()), ctypes.c_uint64(int(cmp_len)), x, y, z, _bins(bins),
         ctypes.c_float(pooling), ctypes.c_void_p(d_out.data_ptr()), ctypes.c_void_p(_stream_handle(stream)))
-    _check(st, "lscomp_decompress_u16_async")
+    _check(st, f"lscomp_decompress_{_suffix(d_out)}_async")
 
 
 _default_ws = {}

@@ -159,3 +159,88 @@ def test_truncated_stream_rejected(lz, ws):
     with pytest.raises(lz.LscompError) as e:
         lz.decompress_into(ws, out, sl - 64, dims, *LOSSLESS, d)
     assert e.value.status == 2
+
+
+# ---------------------------------------------------------------- uint32 twins
+U32_SETTINGS = [LOSSLESS, LOSSY, ((7, 7, 7, 7), 0.3), ((9, 4, 12, 3), 0.5), ((1, 1, 1, 1), 0.0),
+                ((2, 1000, 70000, 1 << 20), 0.8)]
+
+
+def random_stack32(dims, seed, hi=1 << 20):
+    rng = np.random.default_rng(seed)
+    a = rng.integers(0, hi, size=dims, dtype=np.uint32)
+    a[rng.random(dims) < 0.5] = 0
+    a[rng.random(dims) < 0.01] = 0x7FFFFFFF
+    return a
+
+
+@pytest.mark.parametrize("dims", [(1, 8, 8), (2, 13, 21), (3, 37, 53), (2, 17, 1100), (4, 64, 64), (1, 1025, 9)])
+@pytest.mark.parametrize("bins,p", U32_SETTINGS)
+def test_u32_vs_oracle(lz, ws, oracle, dims, bins, p):
+    a = random_stack32(dims, seed=hash((dims, bins, p)) & 0xffff)
+    s_o, rs_o = oracle.compress(a, dims, bins, p, dtype=np.uint32)
+    d_in = torch.from_numpy(a.view(np.int32).ravel()).cuda()
+    out = torch.zeros(lz.max_stream_bytes(dims, 4), dtype=torch.uint8, device="cuda")
+    sl, rs = lz.compress_into(ws, d_in, dims, bins, p, out)
+    assert sl == len(s_o)
+    assert np.array_equal(out[:sl].cpu().numpy(), s_o)
+    dec = torch.full((a.size,), -1, dtype=torch.int32, device="cuda")
+    lz.decompress_into(ws, out, sl, dims, bins, p, dec)
+    d_o = oracle.decompress(s_o, dims, bins, p, dtype=np.uint32)
+    assert np.array_equal(dec.cpu().numpy().view(np.uint32), d_o)
+
+
+def test_u32_vs_reference_build(lz, ws, ref):
+    dims = (8, 128, 96)
+    a = random_stack32(dims, seed=12)
+    d_in = torch.from_numpy(a.view(np.int32).ravel()).cuda()
+    cap = lz.max_stream_bytes(dims, 4)
+    ref_out = torch.zeros(cap, dtype=torch.uint8, device="cuda")
+    for bins, p in (LOSSLESS, LOSSY):
+        ref_out.zero_()
+        rs_ref = ref.compress(d_in.data_ptr(), ref_out.data_ptr(), dims, bins, p, t="u32")
+        torch.cuda.synchronize()
+        out = torch.zeros(cap, dtype=torch.uint8, device="cuda")
+        sl, rs = lz.compress_into(ws, d_in, dims, bins, p, out)
+        assert torch.equal(out[:sl], ref_out[:sl])
+        assert rs == rs_ref
+
+
+def test_u32_rate32_rejected(lz, ws):
+    # a quotient >= 2^31 needs 32 planes; the reference writes a stream its own
+    # decoder misreads, this library reports the range error instead
+    a = np.zeros((1, 8, 8), dtype=np.uint32)
+    a[0, 0, 0] = 0xFFFFFFFF
+    d_in = torch.from_numpy(a.view(np.int32).ravel()).cuda()
+    out = torch.zeros(lz.max_stream_bytes((1, 8, 8), 4), dtype=torch.uint8, device="cuda")
+    with pytest.raises(lz.LscompError) as e:
+        lz.compress_into(ws, d_in, (1, 8, 8), LOSSLESS[0], 1.0, out)
+    assert e.value.status == 6
+    # same value with bin 2 fits in 31 planes
+    sl, _ = lz.compress_into(ws, d_in, (1, 8, 8), (2, 2, 2, 2), 1.0, out)
+    assert out[0].item() & 31 == 31
+
+
+@pytest.mark.parametrize("in_off,out_off", [(1, 0), (3, 4), (5, 12), (0, 8)])
+@pytest.mark.parametrize("dims", [(3, 37, 53), (2, 64, 64), (1, 17, 2051)])
+@pytest.mark.parametrize("bins,p", [LOSSLESS, LOSSY])
+def test_unaligned_pointers(lz, ws, oracle, in_off, out_off, dims, bins, p):
+    """Input starting off a 16-byte boundary (the TMA fetch then copies the
+    ragged ends of the array element by element) and streams at 4-byte offsets."""
+    a = random_stack(dims, seed=21, zero_frac=0.4, hi=3000)
+    n = a.size
+    buf = torch.zeros(n + 16, dtype=torch.int16, device="cuda")
+    buf[in_off:in_off + n] = to_dev(a)
+    d_in = buf[in_off:in_off + n]
+    cap = lz.max_stream_bytes(dims)
+    obuf = torch.zeros(cap + 32, dtype=torch.uint8, device="cuda")
+    out = obuf[out_off:out_off + cap]
+    sl, _ = lz.compress_into(ws, d_in, dims, bins, p, out)
+    s_o, _ = oracle.compress(a, dims, bins, p)
+    assert np.array_equal(out[:sl].cpu().numpy(), s_o)
+    dbuf = torch.full((n + 16,), -1, dtype=torch.int16, device="cuda")
+    dec = dbuf[in_off:in_off + n]
+    lz.decompress_into(ws, out, sl, dims, bins, p, dec)
+    assert np.array_equal(dec.cpu().numpy().view(np.uint16), oracle.decompress(s_o, dims, bins, p))
+    # nothing outside the output range was touched
+    assert int((dbuf[:in_off] != -1).sum()) == 0 and int((dbuf[in_off + n:] != -1).sum()) == 0
