@@ -79,10 +79,13 @@ LSC_HD void lsc_row_values(uint32_t l_lo, uint32_t l_hi, uint32_t h_lo, uint32_t
     w0 = lsc_prmt(l_hi, h_hi, 0x6273u);
 }
 
-// Second step of the 4x4 byte transpose across four threads (after the
-// exchange with the thread two rows away, see the kernels): selectors for
-// the even and the odd member of each pair.
-#define LSC_XP_A_LOW 0x5410u   // keep own bytes 0,1, take partner bytes 0,1
-#define LSC_XP_A_HIGH 0x7632u  // take partner bytes 2,3, keep own bytes 2,3 (partner first)
-#define LSC_XP_B_EVEN 0x6240u
-#define LSC_XP_B_ODD 0x3715u
+// Byte selectors of the 4x4 byte transpose across four threads r = 0..3
+// (see xpose4 in the kernels).  Step A exchanges with thread r^2: threads 0,1
+// keep their bytes 0,1 and take the partner's bytes 0,1; threads 2,3 take the
+// partner's bytes 2,3 and keep their own bytes 2,3.  Step B exchanges with
+// thread r^1 and interleaves single bytes.  Each selector applies to
+// {partner : own}, so one PRMT per step with a per-thread selector.
+#define LSC_XP_A_LOW 0x5410u   // r < 2:  own0 own1 prt0 prt1
+#define LSC_XP_A_HIGH 0x3276u  // r >= 2: prt2 prt3 own2 own3
+#define LSC_XP_B_EVEN 0x6240u  // r even: own0 prt0 own2 prt2
+#define LSC_XP_B_ODD 0x3715u   // r odd:  prt1 own1 prt3 own3

@@ -111,7 +111,9 @@ bool make_codec(const uint32_t bins[4], float p, bool wide, Codec &c, int &layou
         c.binc[k] = (!wide && bins[k] > 65536u) ? 65536u : bins[k];
     }
     c.pool_min = pool_min_zeros(p);
-    if (bins[0] == bins[1] && bins[1] == bins[2] && bins[2] == bins[3])
+    if (bins[0] == 1 && bins[1] == 1 && bins[2] == 1 && bins[3] == 1)
+        layout = BINS_IDENT;
+    else if (bins[0] == bins[1] && bins[1] == bins[2] && bins[2] == bins[3])
         layout = BINS_EQUAL;
     else if (bins[0] <= bins[1] && bins[1] <= bins[2] && bins[2] <= bins[3])
         layout = BINS_MONO;
@@ -187,6 +189,9 @@ int launch_enc_t(const EncArgs<T> &a, int sm_count, cudaStream_t st)
 template <typename T, int VEC>
 int launch_enc_v(const EncArgs<T> &a, int layout, bool pool, int sm, cudaStream_t st)
 {
+    if (layout == BINS_IDENT)
+        return pool ? launch_enc_t<T, VEC, BINS_IDENT, true>(a, sm, st)
+                    : launch_enc_t<T, VEC, BINS_IDENT, false>(a, sm, st);
     if (layout == BINS_EQUAL)
         return pool ? launch_enc_t<T, VEC, BINS_EQUAL, true>(a, sm, st)
                     : launch_enc_t<T, VEC, BINS_EQUAL, false>(a, sm, st);

@@ -35,6 +35,26 @@
 #include "bitplane.h"
 #include "device_prims.cuh"
 
+// Tuning switches (compile-time; the defaults are the measured best on B200):
+//   LSC_WRITERS       writer warps per encoder CTA (1 or 2)
+//   LSC_LOOKBACK      0: 32-wide look-back to the nearest inclusive prefix,
+//                     1: 256-wide look-back bounded by the writer's previous tile
+//   LSC_DEC_HOIST     1: the decoder issues all payload loads of a warp's
+//                     units before transposing any of them
+//   LSC_ENC_WARPS     compute warps per encoder CTA
+#ifndef LSC_WRITERS
+#define LSC_WRITERS 1
+#endif
+#ifndef LSC_LOOKBACK
+#define LSC_LOOKBACK 0
+#endif
+#ifndef LSC_DEC_HOIST
+#define LSC_DEC_HOIST 0
+#endif
+#ifndef LSC_ENC_WARPS
+#define LSC_ENC_WARPS 16  // compute warps per encoder CTA
+#endif
+
 namespace lsc {
 
 constexpr int kThreads = 256;                  // 8 warps per CTA
@@ -47,6 +67,7 @@ constexpr int kStageBytes = 33280;             // >= one tile's input + alignmen
 constexpr int BINS_EQUAL = 0;   // all four bins equal: bin choice is always 3
 constexpr int BINS_MONO = 1;    // x <= y <= z <= w (what the CLI accepts)
 constexpr int BINS_GENERAL = 2; // anything else the host API allows
+constexpr int BINS_IDENT = 3;   // all four bins 1 (the lossless mode): no quantisation
 
 // Per element type: words per 8-value row, plane byte groups, largest rate
 // the 5-bit header field carries, and blocks per tile (4 KB of input per
@@ -367,6 +388,39 @@ __device__ __forceinline__ uint32_t or_all(const Row<uint32_t> &v)
 
 __device__ __forceinline__ uint32_t bitlen(uint32_t v) { return 32u - __clz(v); }
 
+// largest value of the row (16-bit halves compared pairwise with max.u16x2)
+__device__ __forceinline__ uint32_t max2u16(uint32_t a, uint32_t b)
+{
+    uint32_t d;
+    asm("max.u16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+    return d;
+}
+
+__device__ __forceinline__ uint32_t max_all(const Row<uint16_t> &v)
+{
+    const uint32_t m = max2u16(max2u16(v.w[0], v.w[1]), max2u16(v.w[2], v.w[3]));
+    return max(m & 0xffffu, m >> 16);
+}
+
+__device__ __forceinline__ uint32_t max_all(const Row<uint32_t> &v)
+{
+    uint32_t m = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) m = max(m, v.w[i]);
+    return m;
+}
+
+// one value quantised by the chosen bin
+__device__ __forceinline__ uint32_t quant1(uint32_t v, const Codec &c, uint32_t choice, bool wide)
+{
+    if (wide) {
+        const unsigned long long m = c.magic64[choice];
+        return m ? (uint32_t)__umul64hi((unsigned long long)v, m) : v;
+    }
+    const uint32_t m = c.magic[choice];
+    return m ? __umulhi(v, m) : v;
+}
+
 // plane bytes of byte group g (planes 8g..8g+7) of one row: on return lo holds
 // planes 8g+{0,1,2,3} and hi planes 8g+{4,5,6,7}, one byte per plane
 __device__ __forceinline__ void row_planes(const Row<uint16_t> &v, uint32_t g, uint32_t &lo, uint32_t &hi)
@@ -382,16 +436,29 @@ __device__ __forceinline__ void row_planes(const Row<uint32_t> &v, uint32_t g, u
     lsc_transpose8x8(lo, hi);
 }
 
-// inverse of row_planes over all groups: P[g][0] = lo, P[g][1] = hi
-__device__ __forceinline__ void row_values(uint32_t P[][2], Row<uint16_t> &v)
+// inverse of row_planes over all groups: P[g][0] = lo, P[g][1] = hi.
+// Groups at or above wrate (the largest rate in the unit) are zero and
+// need no transpose.
+__device__ __forceinline__ void row_values(uint32_t P[][2], Row<uint16_t> &v, uint32_t wrate)
 {
-    lsc_row_values(P[0][0], P[0][1], P[1][0], P[1][1], v.w[0], v.w[1], v.w[2], v.w[3]);
+    if (wrate > 8u) {
+        lsc_row_values(P[0][0], P[0][1], P[1][0], P[1][1], v.w[0], v.w[1], v.w[2], v.w[3]);
+    } else {
+        uint32_t lo = P[0][0], hi = P[0][1];
+        lsc_transpose8x8(lo, hi);  // low value bytes: lo = q7 q6 q5 q4, hi = q3 q2 q1 q0
+        // the selectors of lsc_row_values with zero high value bytes
+        v.w[3] = __byte_perm(lo, 0u, 0x4051u);
+        v.w[2] = __byte_perm(lo, 0u, 0x6273u);
+        v.w[1] = __byte_perm(hi, 0u, 0x4051u);
+        v.w[0] = __byte_perm(hi, 0u, 0x6273u);
+    }
 }
 
-__device__ __forceinline__ void row_values(uint32_t P[][2], Row<uint32_t> &v)
+__device__ __forceinline__ void row_values(uint32_t P[][2], Row<uint32_t> &v, uint32_t wrate)
 {
 #pragma unroll
-    for (int g = 0; g < 4; g++) lsc_transpose8x8(P[g][0], P[g][1]);  // byte g of v7..v4 / v3..v0
+    for (int g = 0; g < 4; g++)
+        if (wrate > 8u * g) lsc_transpose8x8(P[g][0], P[g][1]);  // byte g of v7..v4 / v3..v0
 #pragma unroll
     for (int k = 0; k < 4; k++) {
         const uint32_t s = (uint32_t)k | ((uint32_t)(k + 4) << 4);
@@ -439,22 +506,35 @@ __device__ __forceinline__ Row<uint32_t> unpool_row(const Row<uint32_t> &q, bool
 }
 
 // 4x4 byte transpose across the lanes j, j+8, j+16, j+24 (r = lane >> 3):
-// lane r ends with byte c = byte r of lane c's input.
-__device__ __forceinline__ uint32_t xpose4(uint32_t x, uint32_t r)
+// lane r ends with byte c = byte r of lane c's input.  The per-lane byte
+// selectors are fixed for a thread and computed once.
+struct XSel {
+    uint32_t a, b;
+};
+
+__device__ __forceinline__ XSel xsel(uint32_t r)
 {
-    uint32_t t = __shfl_xor_sync(0xffffffffu, x, 16);
-    uint32_t z = (r < 2u) ? __byte_perm(x, t, LSC_XP_A_LOW) : __byte_perm(t, x, LSC_XP_A_HIGH);
-    t = __shfl_xor_sync(0xffffffffu, z, 8);
-    return (r & 1u) ? __byte_perm(z, t, LSC_XP_B_ODD) : __byte_perm(z, t, LSC_XP_B_EVEN);
+    XSel s;
+    s.a = r < 2u ? LSC_XP_A_LOW : LSC_XP_A_HIGH;
+    s.b = (r & 1u) ? LSC_XP_B_ODD : LSC_XP_B_EVEN;
+    return s;
+}
+
+__device__ __forceinline__ uint32_t xpose4(uint32_t x, const XSel &s)
+{
+    const uint32_t z = __byte_perm(x, __shfl_xor_sync(0xffffffffu, x, 16), s.a);
+    return __byte_perm(z, __shfl_xor_sync(0xffffffffu, z, 8), s.b);
 }
 
 // ---------------------------------------------------------------- shared state
 // Encoder CTA: kEncWarps compute warps, one producer warp (tile claims and
-// TMA loads) and one writer warp (look-back and write-out), one CTA per SM.
-constexpr int kEncWarps = 16;
-constexpr int kEncThreads = (kEncWarps + 2) * 32;
+// TMA loads) and kWriters writer warps (look-back and write-out, alternate
+// tiles), one CTA per SM.
+constexpr int kEncWarps = LSC_ENC_WARPS;
+constexpr int kWriters = LSC_WRITERS;         // writer warps, taking alternate tiles
+constexpr int kEncThreads = (kEncWarps + 1 + kWriters) * 32;
 constexpr int kProducerWarp = kEncWarps;
-constexpr int kWriterWarp = kEncWarps + 1;
+constexpr int kWriterWarp0 = kEncWarps + 1;
 constexpr int kInStages = 3;                  // input ring (TMA destination)
 constexpr int kStStages = 3;                  // packed-payload ring (write-out source)
 constexpr int kStagingBytes = 32896;          // >= one tile's worst-case payload (32768)
@@ -471,8 +551,11 @@ struct EncSmem {
     uint32_t in_mis[kInStages][8];     // byte misalignment of each range start (mod 16)
     unsigned long long st_tile[kStStages];
     uint32_t st_agg[kStStages];
-    uint32_t br_rel[kMaxTileBlocks];   // whole-row tiles: element offset of block-row g from the tile start
-    uint8_t br_rows[kMaxTileBlocks];   // rows in block-row g
+    // per input slot: whole-row tiles: element offset of block-row g from the
+    // tile start and its row count (chunked tiles: rows in [0]); filled by the
+    // producer warp with the load
+    uint32_t br_rel[kInStages][kMaxTileBlocks];
+    uint8_t br_rows[kInStages][kMaxTileBlocks];
     uint8_t hdr[kMaxTileBlocks];       // header byte per block
     uint32_t off[kMaxTileBlocks];      // payload offset of each block inside the tile
     uint32_t agg;
@@ -679,7 +762,7 @@ __device__ __forceinline__ bool compute_bar_and(bool pred)
 
 // Pass A for one unit: statistics -> header byte (lsCOMP/src/cuLSZ_kernel.cu:898-957).
 // Returns the header byte (same in the 4 lanes of a block).
-template <typename T, int BINS, bool POOL>
+template <typename T, int BINS, bool POOL, bool IDENT>
 __device__ __forceinline__ uint32_t block_header(const Row<T> &A, const Row<T> &B, const Codec &c, uint32_t &range_bad)
 {
     uint32_t choice = 3;
@@ -718,29 +801,30 @@ __device__ __forceinline__ uint32_t block_header(const Row<T> &A, const Row<T> &
         zc += __shfl_xor_sync(0xffffffffu, zc, 16);
         pool = (int)zc >= c.pool_min;
     }
-    uint32_t orv;
-    if (pool) {
-        Row<T> P = pool_rows(A, B);
-        quant(P, c, choice);
-        orv = or_all(P);
+    // rate = bit length of the largest quantised value (cuLSZ_kernel.cu:937-957);
+    // quantisation is monotone, so only the block maximum is divided
+    uint32_t mx;
+    if (IDENT) {
+        mx = pool ? or_all(pool_rows(A, B)) : (or_all(A) | or_all(B));  // same bit length as the max
+        mx |= __shfl_xor_sync(0xffffffffu, mx, 8);
+        mx |= __shfl_xor_sync(0xffffffffu, mx, 16);
     } else {
-        Row<T> qa = A, qb = B;
-        quant(qa, c, choice);
-        quant(qb, c, choice);
-        orv = or_all(qa) | or_all(qb);
+        mx = pool ? max_all(pool_rows(A, B)) : max(max_all(A), max_all(B));
+        mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, 8));
+        mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, 16));
+        mx = quant1(mx, c, choice, sizeof(T) == 4);
     }
-    orv |= __shfl_xor_sync(0xffffffffu, orv, 8);
-    orv |= __shfl_xor_sync(0xffffffffu, orv, 16);
-    const uint32_t rate = bitlen(orv);
+    const uint32_t rate = bitlen(mx);
     range_bad = rate > Elem<T>::kMaxRate;
     return (pool ? 0x80u : 0u) | (choice << 5) | (rate & 0x1fu);
 }
 
 // Pass B for one unit: bit planes (lsCOMP/src/cuLSZ_kernel.cu:1100-1276) of
-// the block whose header is h, stored at dst (shared memory).
-template <typename T>
+// the block whose header is h, stored at dst (shared memory).  IDENT: every
+// bin is 1, values are their own quantisation.
+template <typename T, bool IDENT>
 __device__ __forceinline__ void block_pack(const Row<T> &A0, const Row<T> &B0, uint32_t h, bool active, uint32_t r,
-                                           const Codec &c, uint8_t *dst)
+                                           const XSel &xs, const Codec &c, uint8_t *dst)
 {
     constexpr int NW = Elem<T>::kWords;
     constexpr int NG = Elem<T>::kGroups;
@@ -753,7 +837,7 @@ __device__ __forceinline__ void block_pack(const Row<T> &A0, const Row<T> &B0, u
         // pooled blocks: lane r=0 takes row pair (0,1), r=1 (4,5), r=2 (2,3),
         // r=3 (6,7) -- one pooled byte row each
         Row<T> P = pool_rows(A0, B0);
-        quant(P, c, choice);
+        if (!IDENT) quant(P, c, choice);
         Row<T> V;
 #pragma unroll
         for (int i = 0; i < NW / 2; i++) {
@@ -766,11 +850,11 @@ __device__ __forceinline__ void block_pack(const Row<T> &A0, const Row<T> &B0, u
             A = V;
 #pragma unroll
             for (int i = 0; i < NW; i++) B.w[i] = 0;
-        } else {
+        } else if (!IDENT) {
             quant(A, c, choice);
             quant(B, c, choice);
         }
-    } else {
+    } else if (!IDENT) {
         quant(A, c, choice);
         quant(B, c, choice);
     }
@@ -781,24 +865,25 @@ __device__ __forceinline__ void block_pack(const Row<T> &A0, const Row<T> &B0, u
         uint32_t aL, aH, bL, bH;
         row_planes(A, grp, aL, aH);
         row_planes(B, grp, bL, bH);
-        uint32_t y1 = xpose4(aL, r), y2 = xpose4(bL, r), y3 = xpose4(aH, r), y4 = xpose4(bH, r);
         const uint32_t pl = 8u * grp + r;  // planes pl and pl + 4
+        uint32_t y1 = xpose4(aL, xs), y2 = xpose4(bL, xs);
         if (pool) {
             y1 = __byte_perm(y1, 0, 0x3120);  // row pairs were taken in the order 0,2,1,3
-            y3 = __byte_perm(y3, 0, 0x3120);
             if (active && pl < rate) *reinterpret_cast<uint32_t *>(dst + 4u * pl) = y1;
-            if (active && pl + 4u < rate) *reinterpret_cast<uint32_t *>(dst + 4u * (pl + 4u)) = y3;
-        } else {
+        } else if (active && pl < rate) {
             // block payloads start at multiples of 4 bytes only (a pooled block
             // has 4 bytes per plane), so the plane pairs go out as two words
-            if (active && pl < rate) {
-                *reinterpret_cast<uint32_t *>(dst + 8u * pl) = y1;
-                *reinterpret_cast<uint32_t *>(dst + 8u * pl + 4u) = y2;
-            }
-            if (active && pl + 4u < rate) {
-                *reinterpret_cast<uint32_t *>(dst + 8u * (pl + 4u)) = y3;
-                *reinterpret_cast<uint32_t *>(dst + 8u * (pl + 4u) + 4u) = y4;
-            }
+            *reinterpret_cast<uint32_t *>(dst + 8u * pl) = y1;
+            *reinterpret_cast<uint32_t *>(dst + 8u * pl + 4u) = y2;
+        }
+        if (wrate <= 8u * grp + 4u) break;  // planes 8 grp + 4.. are empty in the whole unit
+        uint32_t y3 = xpose4(aH, xs), y4 = xpose4(bH, xs);
+        if (pool) {
+            y3 = __byte_perm(y3, 0, 0x3120);
+            if (active && pl + 4u < rate) *reinterpret_cast<uint32_t *>(dst + 4u * (pl + 4u)) = y3;
+        } else if (active && pl + 4u < rate) {
+            *reinterpret_cast<uint32_t *>(dst + 8u * (pl + 4u)) = y3;
+            *reinterpret_cast<uint32_t *>(dst + 8u * (pl + 4u) + 4u) = y4;
         }
     }
 }
@@ -809,10 +894,11 @@ __device__ __forceinline__ void block_pack(const Row<T> &A0, const Row<T> &B0, u
 template <typename T, int VEC, int BINS, bool POOL>
 __device__ __forceinline__ void enc_compute(const EncArgs<T> &a, EncSmem &sm)
 {
-    constexpr int UMAX = Elem<T>::kTileBlocks / 8 / kEncWarps;  // units per warp per tile
+    constexpr int UMAX = (Elem<T>::kTileBlocks / 8 + kEncWarps - 1) / kEncWarps;  // units per warp per tile
     const Geom &g = a.g;
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t jb = lane & 7, r = lane >> 3;
+    const XSel xs = xsel(r);
     uint32_t consumed = 0;  // input-ring entries whose load this loop has waited for
     for (uint32_t k = 0;; k++) {
         const int i = (int)(k % kInStages), j = (int)(k % kStStages);
@@ -822,29 +908,19 @@ __device__ __forceinline__ void enc_compute(const EncArgs<T> &a, EncSmem &sm)
         consumed = k + 1;
         const unsigned long long t = sm.in_tile[i];
         if (t >= g.ntiles) {
-            // end of this CTA's tiles: hand the end marker to the writer
-            if (tid == 0 && mbar_wait(&sm.st_empty[j], (m & 1u) ^ 1u, a.ctl)) {
-                sm.st_tile[j] = t;
-                mbar_arrive(&sm.st_full[j]);
+            // end of this CTA's tiles: hand an end marker to every writer
+            if (tid == 0) {
+                for (uint32_t e = 0; e < (uint32_t)kWriters; e++) {
+                    const uint32_t kk = k + e, jj = kk % kStStages, mm = kk / kStStages;
+                    if (!mbar_wait(&sm.st_empty[jj], (mm & 1u) ^ 1u, a.ctl)) break;
+                    sm.st_tile[jj] = t;
+                    mbar_arrive_cnt(&sm.st_full[jj], kEncWarps);
+                }
             }
             break;
         }
         const TileInfo ti = tile_info(g, t);
         const uint8_t *stage = sm.in[i];
-        if (!g.chunked) {
-            if (tid < ti.nbr) {
-                uint32_t nrows, n0;
-                unsigned long long rs = brow_start(g, ti.rho0 + tid, nrows);
-                unsigned long long r0 = brow_start(g, ti.rho0, n0);
-                sm.br_rel[tid] = (uint32_t)((rs - r0) * g.Z);
-                sm.br_rows[tid] = (uint8_t)nrows;
-            }
-        } else if (tid == 0) {
-            uint32_t nrows;
-            brow_start(g, ti.rho0, nrows);
-            sm.br_rows[0] = (uint8_t)nrows;
-        }
-        compute_bar();
 
         // ---- pass A: rows to registers, header bytes
         const uint32_t nunits = (ti.nblk + 7) >> 3;
@@ -858,10 +934,10 @@ __device__ __forceinline__ void enc_compute(const EncArgs<T> &a, EncSmem &sm)
             if (u < nunits) {
                 const uint32_t b = u * 8 + jb;
                 const bool active = b < ti.nblk;
-                SegLoc L = seg_locate<T, true>(g, ti, sm.br_rel, sm.br_rows, stage, sm.in_mis[i], active ? b : 0, r);
+                SegLoc L = seg_locate<T, true>(g, ti, sm.br_rel[i], sm.br_rows[i], stage, sm.in_mis[i], active ? b : 0, r);
                 load_rows<T, VEC>(L, active, r, A[q], B[q]);
                 uint32_t rb;
-                hq[q] = block_header<T, BINS, POOL>(A[q], B[q], a.c, rb);
+                hq[q] = block_header<T, BINS == BINS_IDENT ? BINS_EQUAL : BINS, POOL, BINS == BINS_IDENT>(A[q], B[q], a.c, rb);
                 if (active && r == 0) {
                     sm.hdr[b] = (uint8_t)hq[q];
                     bad |= rb;
@@ -900,15 +976,17 @@ __device__ __forceinline__ void enc_compute(const EncArgs<T> &a, EncSmem &sm)
             if (u < nunits) {
                 const uint32_t b = u * 8 + jb;
                 const bool active = b < ti.nblk;
-                block_pack<T>(A[q], B[q], hq[q], active, r, a.c, st + (active ? sm.off[b] : 0u));
+                block_pack<T, BINS == BINS_IDENT>(A[q], B[q], hq[q], active, r, xs, a.c,
+                                                   st + (active ? sm.off[b] : 0u));
             }
         }
-        compute_bar();
+        // each warp reports its part of the packed tile; the writer waits for all
         if (tid == 0) {
             sm.st_tile[j] = t;
             sm.st_agg[j] = sm.agg;
-            mbar_arrive(&sm.st_full[j]);
         }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&sm.st_full[j]);
     }
     if (tid == 0) sm.consumed = consumed;
 }
@@ -925,11 +1003,27 @@ __device__ __forceinline__ void enc_producer(const EncArgs<T> &a, EncSmem &sm)
         bool ok = mbar_wait(&sm.in_empty[i], (n & 1u) ^ 1u, a.ctl);
         if (!__all_sync(0xffffffffu, ok)) break;
         unsigned long long t = 0;
-        if (lane == 0) {
-            t = aborted(a.ctl) ? a.g.ntiles : atomicAdd(&a.ctl->ticket, 1ull);
-            enc_issue<T>(a, sm, i, t);
-        }
+        if (lane == 0) t = aborted(a.ctl) ? a.g.ntiles : atomicAdd(&a.ctl->ticket, 1ull);
         t = __shfl_sync(0xffffffffu, t, 0);
+        if (t < a.g.ntiles) {
+            // block-row table of the tile for the compute warps
+            const Geom &g = a.g;
+            const TileInfo ti = tile_info(g, t);
+            uint32_t n0;
+            const unsigned long long r0 = brow_start(g, ti.rho0, n0);
+            if (!g.chunked) {
+                for (uint32_t q = lane; q < ti.nbr; q += 32) {
+                    uint32_t nrows;
+                    const unsigned long long rs = brow_start(g, ti.rho0 + q, nrows);
+                    sm.br_rel[i][q] = (uint32_t)((rs - r0) * g.Z);
+                    sm.br_rows[i][q] = (uint8_t)nrows;
+                }
+            } else if (lane == 0) {
+                sm.br_rows[i][0] = (uint8_t)n0;
+            }
+        }
+        __syncwarp();
+        if (lane == 0) enc_issue<T>(a, sm, i, t);  // arrives on in_full after the table
         if (t >= a.g.ntiles) {
             k++;
             break;
@@ -938,15 +1032,18 @@ __device__ __forceinline__ void enc_producer(const EncArgs<T> &a, EncSmem &sm)
     if (lane == 0) sm.issued = k;
 }
 
-// Writer warp: for each packed tile, the decoupled look-back for its stream
-// offset, publication of the inclusive prefix, and the copy of the payload
-// from the ring to the stream.
+// Writer warp w: for the CTA's tiles k = w, w + kWriters, ..., the look-back
+// for the tile's stream offset (bounded below by this writer's previous
+// tile, whose inclusive prefix it published itself), publication of the
+// inclusive prefix, and the copy of the packed payload to the stream.
 template <typename T>
-__device__ __forceinline__ void enc_writer(const EncArgs<T> &a, EncSmem &sm)
+__device__ __forceinline__ void enc_writer(const EncArgs<T> &a, EncSmem &sm, uint32_t w)
 {
     const Geom &g = a.g;
     const uint32_t lane = threadIdx.x & 31;
-    for (uint32_t k = 0;; k++) {
+    long long floor = -1;               // this writer's previous tile
+    unsigned long long floor_incl = 0;  // and its inclusive prefix
+    for (uint32_t k = w;; k += kWriters) {
         const int j = (int)(k % kStStages);
         const uint32_t m = k / kStStages;
         bool ok = mbar_wait(&sm.st_full[j], m & 1u, a.ctl);
@@ -955,12 +1052,18 @@ __device__ __forceinline__ void enc_writer(const EncArgs<T> &a, EncSmem &sm)
         if (t >= g.ntiles) break;
         const uint32_t agg = sm.st_agg[j];
         unsigned long long excl = 0;
-        bool lok = true;
         if (t > 0) {
+            bool lok = true;
+#if LSC_LOOKBACK
+            excl = lookback_floor(a.state, (long long)t, floor, floor_incl, a.epoch, a.ctl, lok);
+#else
             excl = lookback_warp(a.state, t, a.epoch, a.ctl, lok);
+#endif
             if (!lok) break;
             if (lane == 0) st_release_u64(a.state + t, make_state(a.epoch, kFlagIncl, excl + agg));
         }
+        floor = (long long)t;
+        floor_incl = excl + agg;
         if (g.R + excl + agg > a.cap) {
             if (lane == 0) raise_error(a.ctl, DEV_ERR_CAPACITY);
             break;
@@ -973,6 +1076,7 @@ __device__ __forceinline__ void enc_writer(const EncArgs<T> &a, EncSmem &sm)
         if (head > agg) head = agg;
         if (lane < head / 4u) reinterpret_cast<uint32_t *>(dst)[lane] = reinterpret_cast<const uint32_t *>(src)[lane];
         const uint32_t nbody = (agg - head) / 16u;
+#pragma unroll 4
         for (uint32_t c = lane; c < nbody; c += 32) {
             const uint32_t *s4 = reinterpret_cast<const uint32_t *>(src + head + 16u * c);
             *reinterpret_cast<uint4 *>(dst + head + 16u * c) = make_uint4(s4[0], s4[1], s4[2], s4[3]);
@@ -1008,7 +1112,7 @@ __global__ void __launch_bounds__(kEncThreads, 1) enc_kernel(const EncArgs<T> a)
             mbar_init(&sm.in_empty[s], kEncWarps);
         }
         for (int s = 0; s < kStStages; s++) {
-            mbar_init(&sm.st_full[s], 1);
+            mbar_init(&sm.st_full[s], kEncWarps);
             mbar_init(&sm.st_empty[s], 1);
         }
         sm.range_err = 0;
@@ -1022,7 +1126,7 @@ __global__ void __launch_bounds__(kEncThreads, 1) enc_kernel(const EncArgs<T> a)
     else if (warp == (uint32_t)kProducerWarp)
         enc_producer<T>(a, sm);
     else
-        enc_writer<T>(a, sm);
+        enc_writer<T>(a, sm, warp - (uint32_t)kWriterWarp0);
     __syncthreads();
     // After an error a load may still be in flight into a slot nobody
     // consumed; it must land before the CTA's shared memory is released.
@@ -1089,20 +1193,110 @@ __global__ void __launch_bounds__(kThreads) dec_offsets_kernel(const DecArgs<T> 
     }
 }
 
+// Plane words of one block for this lane (planes 8 grp + r and 8 grp + r + 4;
+// words 1 and 3 hold rows 4-7 of a plain block).  Loads only planes < rate.
+template <typename T>
+__device__ __forceinline__ void dec_load(const uint8_t *src, uint32_t h, uint32_t r, uint32_t Y[][4])
+{
+    constexpr int NG = Elem<T>::kGroups;
+    const bool pool = (h & 0x80u) != 0;
+    const uint32_t rate = h & 0x1fu;
+#pragma unroll
+    for (int grp = 0; grp < NG; grp++) {
+        Y[grp][0] = Y[grp][1] = Y[grp][2] = Y[grp][3] = 0;
+        const uint32_t pl = 8u * grp + r;
+        if (pool) {
+            if (pl < rate) Y[grp][0] = *reinterpret_cast<const uint32_t *>(src + 4u * pl);
+            if (pl + 4u < rate) Y[grp][2] = *reinterpret_cast<const uint32_t *>(src + 4u * (pl + 4u));
+        } else {
+            if (pl < rate) {
+                Y[grp][0] = *reinterpret_cast<const uint32_t *>(src + 8u * pl);
+                Y[grp][1] = *reinterpret_cast<const uint32_t *>(src + 8u * pl + 4u);
+            }
+            if (pl + 4u < rate) {
+                Y[grp][2] = *reinterpret_cast<const uint32_t *>(src + 8u * (pl + 4u));
+                Y[grp][3] = *reinterpret_cast<const uint32_t *>(src + 8u * (pl + 4u) + 4u);
+            }
+        }
+    }
+}
+
+// Values of one unit from its plane words: transposes back, pooled rows
+// expanded, de-quantised, stored to rows r and r+4 of block b.
+template <typename T, int VEC>
+__device__ __forceinline__ void dec_unit(const DecArgs<T> &a, const TileInfo &ti, const DecSmem &sm, uint32_t Y[][4],
+                                         uint32_t h, uint32_t b, uint32_t r, unsigned long long ebase)
+{
+    constexpr int NW = Elem<T>::kWords;
+    constexpr int NG = Elem<T>::kGroups;
+    const Geom &g = a.g;
+    const bool even = (r & 1u) == 0;
+    const bool active = b < ti.nblk;
+    SegLoc L = seg_locate<T, false>(g, ti, sm.br_rel, sm.br_rows, nullptr, nullptr, active ? b : 0, r);
+    const bool pool = (h & 0x80u) != 0;
+    const uint32_t bin = a.c.bins[(h >> 5) & 3u];
+    const uint32_t wrate = __reduce_max_sync(0xffffffffu, h & 0x1fu);
+    const XSel xs = xsel(r);
+    // plane bytes per byte group, back in row order: [grp][0/1] = lo/hi half
+    // of row r (PA) and of row r+4 (PB); groups and halves above the unit's
+    // largest rate stay zero without any shuffles
+    uint32_t PA[NG][2], PB[NG][2];
+#pragma unroll
+    for (int grp = 0; grp < NG; grp++) {
+        PA[grp][0] = PA[grp][1] = PB[grp][0] = PB[grp][1] = 0;
+        if (wrate <= 8u * grp) continue;
+        uint32_t y1 = Y[grp][0];
+        if (pool) y1 = __byte_perm(y1, 0, 0x3120);  // undo the row-pair order 0,2,1,3
+        PA[grp][0] = xpose4(y1, xs);
+        PB[grp][0] = xpose4(Y[grp][1], xs);
+        if (wrate <= 8u * grp + 4u) continue;
+        uint32_t y3 = Y[grp][2];
+        if (pool) y3 = __byte_perm(y3, 0, 0x3120);
+        PA[grp][1] = xpose4(y3, xs);
+        PB[grp][1] = xpose4(Y[grp][3], xs);
+    }
+    Row<T> A, B;
+    row_values(PA, A, wrate);
+    row_values(PB, B, wrate);
+    if (__any_sync(0xffffffffu, active && pool)) {
+        // a pooled lane holds the 8 pooled values of its row pair: 4 of the
+        // first row, then 4 of the second.  Even lanes keep the first row and
+        // send the second; odd lanes the reverse.
+        Row<T> Q;
+#pragma unroll
+        for (int i = 0; i < NW / 2; i++) {
+            const uint32_t t0 = __shfl_xor_sync(0xffffffffu, even ? A.w[NW / 2 + i] : A.w[i], 8);
+            Q.w[i] = even ? A.w[i] : t0;                    // row r
+            Q.w[NW / 2 + i] = even ? t0 : A.w[NW / 2 + i];  // row r+4
+        }
+        if (pool) {
+            A = unpool_row(Q, false, bin);
+            B = unpool_row(Q, true, bin);
+        }
+    }
+    if (!pool) {
+        dequant(A, bin);
+        dequant(B, bin);
+    }
+    if (active) {
+        T *rowA = a.out + ebase + L.growA;
+        if (r < L.nrows) store8<VEC>(rowA, A, L.ncols);
+        if (r + 4 < L.nrows) store8<VEC>(rowA + 4ull * g.Z, B, L.ncols);
+    }
+}
+
 // One CTA per tile: header bytes -> in-tile offsets -> plane words of each
 // block -> values scattered to the output rows
 // (lsCOMP/src/cuLSZ_kernel.cu:1440-1640).  Every element of the tile is
 // written, zeros for blocks of rate 0.
 template <typename T, int VEC>
-__global__ void __launch_bounds__(kThreads, 4) dec_kernel(const DecArgs<T> a)
+__global__ void __launch_bounds__(kThreads, LSC_DEC_HOIST ? 3 : 4) dec_kernel(const DecArgs<T> a)
 {
-    constexpr int NW = Elem<T>::kWords;
     constexpr int NG = Elem<T>::kGroups;
     __shared__ DecSmem sm;
     const Geom &g = a.g;
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t jb = lane & 7, r = lane >> 3;
-    const bool even = (r & 1u) == 0;
     const unsigned long long t = blockIdx.x;
     if (t >= g.ntiles) return;
 
@@ -1139,74 +1333,38 @@ __global__ void __launch_bounds__(kThreads, 4) dec_kernel(const DecArgs<T> a)
     const uint8_t *const pay = a.in + g.R + sm.base;
     const unsigned long long ebase = row0 * g.Z;  // element index of the tile's first row
     const uint32_t nunits = (ti.nblk + 7) >> 3;
+#if LSC_DEC_HOIST
+    // all plane words of the warp's units first, so their loads overlap
+    constexpr int UMAX = Elem<T>::kTileBlocks / 8 / kWarps;  // units per warp per tile
+    uint32_t Y[UMAX][NG][4];
+    uint32_t hq[UMAX];
+#pragma unroll
+    for (int q = 0; q < UMAX; q++) {
+        const uint32_t u = warp + (uint32_t)q * kWarps;
+        hq[q] = 0;
+        if (u < nunits) {
+            const uint32_t b = u * 8 + jb;
+            const bool active = b < ti.nblk;
+            hq[q] = active ? sm.hdr[b] : 0u;
+            dec_load<T>(pay + (active ? sm.off[b] : 0u), hq[q], r, Y[q]);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < UMAX; q++) {
+        const uint32_t u = warp + (uint32_t)q * kWarps;
+        if (u < nunits)
+            dec_unit<T, VEC>(a, ti, sm, Y[q], hq[q], u * 8 + jb, r, ebase);
+    }
+#else
     for (uint32_t u = warp; u < nunits; u += kWarps) {
         const uint32_t b = u * 8 + jb;
         const bool active = b < ti.nblk;
-        SegLoc L = seg_locate<T, false>(g, ti, sm.br_rel, sm.br_rows, nullptr, nullptr, active ? b : 0, r);
         const uint32_t h = active ? sm.hdr[b] : 0u;
-        const bool pool = (h & 0x80u) != 0;
-        const uint32_t rate = h & 0x1fu;
-        const uint32_t bin = a.c.bins[(h >> 5) & 3u];
-        const uint8_t *src = pay + (active ? sm.off[b] : 0u);
-        const uint32_t wrate = __reduce_max_sync(0xffffffffu, rate);
-        // plane bytes per byte group, back in row order: [grp][0/1] = lo/hi
-        // half of row r (PA) and of row r+4 (PB)
-        uint32_t PA[NG][2], PB[NG][2];
-#pragma unroll
-        for (uint32_t grp = 0; grp < (uint32_t)NG; grp++) {
-            PA[grp][0] = PA[grp][1] = PB[grp][0] = PB[grp][1] = 0;
-            if (wrate <= 8u * grp) continue;
-            const uint32_t pl = 8u * grp + r;
-            uint32_t y1 = 0, y2 = 0, y3 = 0, y4 = 0;
-            if (pool) {
-                if (pl < rate) y1 = *reinterpret_cast<const uint32_t *>(src + 4u * pl);
-                if (pl + 4u < rate) y3 = *reinterpret_cast<const uint32_t *>(src + 4u * (pl + 4u));
-                y1 = __byte_perm(y1, 0, 0x3120);
-                y3 = __byte_perm(y3, 0, 0x3120);
-            } else {
-                if (pl < rate) {
-                    y1 = *reinterpret_cast<const uint32_t *>(src + 8u * pl);
-                    y2 = *reinterpret_cast<const uint32_t *>(src + 8u * pl + 4u);
-                }
-                if (pl + 4u < rate) {
-                    y3 = *reinterpret_cast<const uint32_t *>(src + 8u * (pl + 4u));
-                    y4 = *reinterpret_cast<const uint32_t *>(src + 8u * (pl + 4u) + 4u);
-                }
-            }
-            PA[grp][0] = xpose4(y1, r);
-            PB[grp][0] = xpose4(y2, r);
-            PA[grp][1] = xpose4(y3, r);
-            PB[grp][1] = xpose4(y4, r);
-        }
-        Row<T> A, B;
-        row_values(PA, A);
-        row_values(PB, B);
-        if (__any_sync(0xffffffffu, active && pool)) {
-            // a pooled lane holds the 8 pooled values of its row pair: 4 of
-            // the first row, then 4 of the second.  Even lanes keep the
-            // first row and send the second; odd lanes the reverse.
-            Row<T> Q;
-#pragma unroll
-            for (int i = 0; i < NW / 2; i++) {
-                const uint32_t t0 = __shfl_xor_sync(0xffffffffu, even ? A.w[NW / 2 + i] : A.w[i], 8);
-                Q.w[i] = even ? A.w[i] : t0;                    // row r
-                Q.w[NW / 2 + i] = even ? t0 : A.w[NW / 2 + i];  // row r+4
-            }
-            if (pool) {
-                A = unpool_row(Q, false, bin);
-                B = unpool_row(Q, true, bin);
-            }
-        }
-        if (!pool) {
-            dequant(A, bin);
-            dequant(B, bin);
-        }
-        if (active) {
-            T *rowA = a.out + ebase + L.growA;
-            if (r < L.nrows) store8<VEC>(rowA, A, L.ncols);
-            if (r + 4 < L.nrows) store8<VEC>(rowA + 4ull * g.Z, B, L.ncols);
-        }
+        uint32_t Y[NG][4];
+        dec_load<T>(pay + (active ? sm.off[b] : 0u), h, r, Y);
+        dec_unit<T, VEC>(a, ti, sm, Y, h, b, r, ebase);
     }
+#endif
 }
 
 }  // namespace lsc

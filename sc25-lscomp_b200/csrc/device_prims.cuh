@@ -68,6 +68,11 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar)
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive_cnt(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes)
 {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
@@ -210,6 +215,87 @@ __device__ __forceinline__ unsigned long long lookback_warp(const unsigned long 
             }
         }
         __nanosleep(32);
+    }
+    return excl;
+}
+
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long *p)
+{
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Decoupled look-back with a known floor: the exclusive prefix of `tile`
+// from the state words of tiles floor+1 .. tile-1 plus the inclusive prefix
+// `floor_incl` of tile `floor` (< tile), which the caller already holds
+// (floor = -1, floor_incl = 0 to walk from the start).  A walk stops early
+// at a nearer inclusive word.  Each round reads 8 consecutive words per lane,
+// 256 tiles per round trip.  Flag and value share one 64-bit word, so relaxed
+// loads suffice.  Run by one full warp; ok = false on timeout or abort.
+constexpr int kLookPerLane = 8;
+
+__device__ __forceinline__ unsigned long long lookback_floor(const unsigned long long *state, long long tile,
+                                                             long long floor, unsigned long long floor_incl,
+                                                             uint32_t epoch, LaunchCtl *ctl, bool &ok)
+{
+    const uint32_t lane = threadIdx.x & 31;
+    unsigned long long excl = 0;
+    long long top = tile - 1;
+    unsigned long long t0 = 0;
+    uint32_t spins = 0;
+    ok = true;
+    for (;;) {
+        uint32_t fl[kLookPerLane];
+        unsigned long long v[kLookPerLane];
+#pragma unroll
+        for (int q = 0; q < kLookPerLane; q++) {
+            const long long idx = top - (long long)(kLookPerLane * lane + q);
+            if (idx > floor) {
+                const unsigned long long w = ld_relaxed_u64(state + idx);
+                const bool fresh = (uint32_t)(w >> kEpochShift) == epoch;
+                fl[q] = fresh ? (uint32_t)((w >> kFlagShift) & 3u) : 0u;
+                v[q] = w & kValueMask;
+            } else {
+                fl[q] = kFlagIncl;  // the floor itself (entries past it are never reached)
+                v[q] = idx == floor ? floor_incl : 0ull;
+            }
+        }
+        uint32_t qi = kLookPerLane, qv = kLookPerLane;  // first inclusive / first missing entry
+#pragma unroll
+        for (int q = kLookPerLane - 1; q >= 0; q--) {
+            if (fl[q] == kFlagIncl) qi = (uint32_t)q;
+            if (fl[q] == 0u) qv = (uint32_t)q;
+        }
+        const uint32_t inclm = __ballot_sync(0xffffffffu, qi < (uint32_t)kLookPerLane);
+        const uint32_t first = inclm ? (uint32_t)(__ffs(inclm) - 1) : 32u;
+        const bool missing = (lane < first && qv < (uint32_t)kLookPerLane) || (lane == first && qv < qi);
+        if (!__any_sync(0xffffffffu, missing)) {
+            unsigned long long part = 0;
+#pragma unroll
+            for (int q = 0; q < kLookPerLane; q++)
+                if (lane < first || (lane == first && (uint32_t)q <= qi)) part += v[q];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+            excl += part;
+            if (inclm) break;
+            top -= 32 * kLookPerLane;
+            continue;
+        }
+        // a tile in range has not published yet: back off, bounded
+        if (spins == 0) t0 = global_ns();
+        ++spins;
+        if ((spins & 15u) == 0) {
+            bool stop = false;
+            if (lane == 0) stop = aborted(ctl) || (global_ns() - t0 > kWaitLimitNs);
+            stop = __shfl_sync(0xffffffffu, stop, 0);
+            if (stop) {
+                if (lane == 0) raise_error(ctl, DEV_ERR_TIMEOUT);
+                ok = false;
+                return 0;
+            }
+        }
+        __nanosleep(64);
     }
     return excl;
 }

@@ -24,7 +24,8 @@ from typing import Optional, Sequence, Tuple
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "liblscomp.so")
+# LSCOMP_LIBRARY selects another build of the same library (tuning variants)
+LIB_PATH = os.environ.get("LSCOMP_LIBRARY", os.path.join(_HERE, "liblscomp.so"))
 SYNTH_PATH = os.path.join(_HERE, "liblscomp_synth.so")
 
 STATUS = {
