@@ -172,18 +172,25 @@ int ctas_per_sm(K kernel, size_t smem)
     return n > 0 ? n : 1;
 }
 
-template <typename T, int VEC, int BINS, bool POOL>
-int launch_enc_t(const EncArgs<T> &a, int sm_count, cudaStream_t st)
+template <typename T, int VEC, int BINS, bool POOL, int GRP, int WPG>
+int launch_enc_w(const EncArgs<T> &a, int sm_count, cudaStream_t st)
 {
-    auto k = enc_kernel<T, VEC, BINS, POOL>;
+    auto k = enc_kernel<T, VEC, BINS, POOL, GRP, WPG>;
     const size_t smem = sizeof(EncSmem);
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     // persistent: one CTA per SM (the CTA holds ~200 KB of rings)
     unsigned long long grid = (unsigned long long)sm_count;
     if (grid > a.g.ntiles) grid = a.g.ntiles;
-    k<<<(unsigned)grid, kEncThreads, smem, st>>>(a);
+    k<<<(unsigned)grid, EncShape<GRP, WPG>::kThreads, smem, st>>>(a);
     g_launches.fetch_add(1);
     return cuda_status(cudaGetLastError());
+}
+
+// Compute warps per encoder CTA: LSC_ENC_GROUPS groups of LSC_ENC_WPG warps.
+template <typename T, int VEC, int BINS, bool POOL>
+int launch_enc_t(const EncArgs<T> &a, int sm_count, cudaStream_t st)
+{
+    return launch_enc_w<T, VEC, BINS, POOL, LSC_ENC_GROUPS, LSC_ENC_WPG>(a, sm_count, st);
 }
 
 template <typename T, int VEC>

@@ -41,7 +41,8 @@
 //                     1: 256-wide look-back bounded by the writer's previous tile
 //   LSC_DEC_HOIST     1: the decoder issues all payload loads of a warp's
 //                     units before transposing any of them
-//   LSC_ENC_WARPS     compute warps per encoder CTA
+//   LSC_ENC_GROUPS    compute groups per encoder CTA (tiles in flight)
+//   LSC_ENC_WPG       warps per compute group
 #ifndef LSC_WRITERS
 #define LSC_WRITERS 1
 #endif
@@ -51,8 +52,11 @@
 #ifndef LSC_DEC_HOIST
 #define LSC_DEC_HOIST 0
 #endif
-#ifndef LSC_ENC_WARPS
-#define LSC_ENC_WARPS 16  // compute warps per encoder CTA
+#ifndef LSC_ENC_GROUPS
+#define LSC_ENC_GROUPS 2  // independent compute groups per encoder CTA
+#endif
+#ifndef LSC_ENC_WPG
+#define LSC_ENC_WPG 8     // warps per compute group
 #endif
 
 namespace lsc {
@@ -527,18 +531,21 @@ __device__ __forceinline__ uint32_t xpose4(uint32_t x, const XSel &s)
 }
 
 // ---------------------------------------------------------------- shared state
-// Encoder CTA: kEncWarps compute warps, one producer warp (tile claims and
-// TMA loads) and kWriters writer warps (look-back and write-out, alternate
-// tiles), one CTA per SM.
-constexpr int kEncWarps = LSC_ENC_WARPS;
+// Encoder CTA: GRP x WPG compute warps in independent groups, one producer
+// warp (tile claims and TMA loads) and kWriters writer warps (look-back and
+// write-out, alternate tiles), one CTA per SM.
 constexpr int kWriters = LSC_WRITERS;         // writer warps, taking alternate tiles
-constexpr int kEncThreads = (kEncWarps + 1 + kWriters) * 32;
-constexpr int kProducerWarp = kEncWarps;
-constexpr int kWriterWarp0 = kEncWarps + 1;
+template <int GRP, int WPG> struct EncShape {
+    static constexpr int kCompute = GRP * WPG;
+    static constexpr int kThreads = (kCompute + 1 + kWriters) * 32;
+    static constexpr int kProducerWarp = kCompute;
+    static constexpr int kWriterWarp0 = kCompute + 1;
+};
 constexpr int kInStages = 3;                  // input ring (TMA destination)
 constexpr int kStStages = 3;                  // packed-payload ring (write-out source)
 constexpr int kStagingBytes = 32896;          // >= one tile's worst-case payload (32768)
-constexpr uint32_t kComputeBarrier = 1;       // named barrier of the compute warps
+constexpr uint32_t kComputeBarrier = 1;       // first named barrier of the compute groups
+constexpr int kMaxGroups = 2;
 
 struct EncSmem {
     alignas(128) uint8_t in[kInStages][kStageBytes];
@@ -556,12 +563,10 @@ struct EncSmem {
     // producer warp with the load
     uint32_t br_rel[kInStages][kMaxTileBlocks];
     uint8_t br_rows[kInStages][kMaxTileBlocks];
-    uint8_t hdr[kMaxTileBlocks];       // header byte per block
-    uint32_t off[kMaxTileBlocks];      // payload offset of each block inside the tile
-    uint32_t agg;
-    uint32_t range_err;
-    uint32_t consumed;                 // input-ring entries the compute warps took
-    uint32_t issued;                   // input-ring entries the producer filled
+    uint8_t hdr[kMaxGroups][kMaxTileBlocks];   // per compute group: header byte per block
+    uint32_t off[kMaxGroups][kMaxTileBlocks];  // payload offset of each block inside the tile
+    uint32_t agg[kMaxGroups];
+    uint32_t issued;                           // input-ring entries the producer filled
 };
 
 struct DecSmem {
@@ -744,9 +749,9 @@ __device__ __forceinline__ void load_rows(const SegLoc &L, bool active, uint32_t
     }
 }
 
-__device__ __forceinline__ void compute_bar() { asm volatile("bar.sync %0, %1;" ::"r"(kComputeBarrier), "r"(kEncWarps * 32) : "memory"); }
-
-__device__ __forceinline__ bool compute_bar_and(bool pred)
+// Named barrier of one compute group (id, thread count), with the AND of a
+// predicate over the group's threads.
+__device__ __forceinline__ bool group_bar_and(uint32_t id, uint32_t nthreads, bool pred)
 {
     uint32_t r;
     asm volatile(
@@ -755,7 +760,7 @@ __device__ __forceinline__ bool compute_bar_and(bool pred)
         "bar.red.and.pred q, %2, %3, p;\n\t"
         "selp.u32 %0, 1, 0, q;\n\t}"
         : "=r"(r)
-        : "r"((uint32_t)pred), "r"(kComputeBarrier), "r"(kEncWarps * 32)
+        : "r"((uint32_t)pred), "r"(id), "r"(nthreads)
         : "memory");
     return r != 0;
 }
@@ -888,34 +893,35 @@ __device__ __forceinline__ void block_pack(const Row<T> &A0, const Row<T> &B0, u
     }
 }
 
-// Compute warps: per tile, pass A from the input ring into registers and
+// Compute warps, in GRP independent groups of WPG warps: group g takes the
+// CTA's tiles k = g, g + GRP, ..., so several tiles are in flight at once
+// and the dependent steps of one tile (reductions, scan, barriers) overlap
+// with another's.  Per tile: pass A from the input ring into registers and
 // header bytes, tile scan and aggregate publication, pass B into the
 // payload ring.
-template <typename T, int VEC, int BINS, bool POOL>
+template <typename T, int VEC, int BINS, bool POOL, int GRP, int WPG>
 __device__ __forceinline__ void enc_compute(const EncArgs<T> &a, EncSmem &sm)
 {
-    constexpr int UMAX = (Elem<T>::kTileBlocks / 8 + kEncWarps - 1) / kEncWarps;  // units per warp per tile
+    constexpr int UMAX = (Elem<T>::kTileBlocks / 8 + WPG - 1) / WPG;  // units per warp per tile
     const Geom &g = a.g;
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t grp = warp / WPG, wg = warp % WPG, gtid = tid - grp * WPG * 32;
+    const uint32_t barid = kComputeBarrier + grp;
     const uint32_t jb = lane & 7, r = lane >> 3;
     const XSel xs = xsel(r);
-    uint32_t consumed = 0;  // input-ring entries whose load this loop has waited for
-    for (uint32_t k = 0;; k++) {
+    uint8_t *const hdr = sm.hdr[grp];
+    uint32_t *const off = sm.off[grp];
+    for (uint32_t k = grp;; k += GRP) {
         const int i = (int)(k % kInStages), j = (int)(k % kStStages);
         const uint32_t n = k / kInStages, m = k / kStStages;
         bool ok = mbar_wait(&sm.in_full[i], n & 1u, a.ctl);
-        if (!compute_bar_and(ok)) break;
-        consumed = k + 1;
+        if (!group_bar_and(barid, WPG * 32, ok)) break;
         const unsigned long long t = sm.in_tile[i];
         if (t >= g.ntiles) {
-            // end of this CTA's tiles: hand an end marker to every writer
-            if (tid == 0) {
-                for (uint32_t e = 0; e < (uint32_t)kWriters; e++) {
-                    const uint32_t kk = k + e, jj = kk % kStStages, mm = kk / kStStages;
-                    if (!mbar_wait(&sm.st_empty[jj], (mm & 1u) ^ 1u, a.ctl)) break;
-                    sm.st_tile[jj] = t;
-                    mbar_arrive_cnt(&sm.st_full[jj], kEncWarps);
-                }
+            // end of this CTA's tiles: hand an end marker to the writer
+            if (gtid == 0 && mbar_wait(&sm.st_empty[j], (m & 1u) ^ 1u, a.ctl)) {
+                sm.st_tile[j] = t;
+                mbar_arrive_cnt(&sm.st_full[j], WPG);
             }
             break;
         }
@@ -929,7 +935,7 @@ __device__ __forceinline__ void enc_compute(const EncArgs<T> &a, EncSmem &sm)
         uint32_t bad = 0;
 #pragma unroll
         for (int q = 0; q < UMAX; q++) {
-            const uint32_t u = warp + (uint32_t)q * kEncWarps;
+            const uint32_t u = wg + (uint32_t)q * WPG;
             hq[q] = 0;
             if (u < nunits) {
                 const uint32_t b = u * 8 + jb;
@@ -939,64 +945,62 @@ __device__ __forceinline__ void enc_compute(const EncArgs<T> &a, EncSmem &sm)
                 uint32_t rb;
                 hq[q] = block_header<T, BINS == BINS_IDENT ? BINS_EQUAL : BINS, POOL, BINS == BINS_IDENT>(A[q], B[q], a.c, rb);
                 if (active && r == 0) {
-                    sm.hdr[b] = (uint8_t)hq[q];
+                    hdr[b] = (uint8_t)hq[q];
                     bad |= rb;
                 }
             }
         }
-        if (bad) sm.range_err = 1;
         __syncwarp();
         if (lane == 0) mbar_arrive(&sm.in_empty[i]);  // the input slot may be refilled
-        compute_bar();
-        if (sm.range_err) {
+        if (!group_bar_and(barid, WPG * 32, bad == 0)) {
             // a uint32 quotient >= 2^31 needs 32 planes, which the 5-bit rate
             // field cannot hold
-            if (tid == 0) raise_error(a.ctl, DEV_ERR_RANGE);
+            if (gtid == 0) raise_error(a.ctl, DEV_ERR_RANGE);
             break;
         }
 
         // ---- tile scan; the aggregate goes out before anything waits on the writer
-        if (warp == 0) {
-            const uint32_t agg = tile_scan(sm.hdr, sm.off, ti.nblk);
+        if (wg == 0) {
+            const uint32_t agg = tile_scan(hdr, off, ti.nblk);
             if (lane == 0) {
-                sm.agg = agg;
+                sm.agg[grp] = agg;
                 st_release_u64(a.state + t, make_state(a.epoch, t == 0 ? kFlagIncl : kFlagAgg, agg));
             }
         }
-        for (uint32_t b = tid; b < ti.nblk; b += kEncWarps * 32) a.out[ti.k0 + b] = sm.hdr[b];
+        for (uint32_t b = gtid; b < ti.nblk; b += WPG * 32) a.out[ti.k0 + b] = hdr[b];
         bool free_ok = true;
-        if (tid == 0) free_ok = mbar_wait(&sm.st_empty[j], (m & 1u) ^ 1u, a.ctl);
-        if (!compute_bar_and(free_ok)) break;
+        if (gtid == 0) free_ok = mbar_wait(&sm.st_empty[j], (m & 1u) ^ 1u, a.ctl);
+        if (!group_bar_and(barid, WPG * 32, free_ok)) break;
 
         // ---- pass B: pack from registers into the payload ring
         uint8_t *const st = sm.st[j];
 #pragma unroll
         for (int q = 0; q < UMAX; q++) {
-            const uint32_t u = warp + (uint32_t)q * kEncWarps;
+            const uint32_t u = wg + (uint32_t)q * WPG;
             if (u < nunits) {
                 const uint32_t b = u * 8 + jb;
                 const bool active = b < ti.nblk;
                 block_pack<T, BINS == BINS_IDENT>(A[q], B[q], hq[q], active, r, xs, a.c,
-                                                   st + (active ? sm.off[b] : 0u));
+                                                   st + (active ? off[b] : 0u));
             }
         }
         // each warp reports its part of the packed tile; the writer waits for all
-        if (tid == 0) {
+        if (gtid == 0) {
             sm.st_tile[j] = t;
-            sm.st_agg[j] = sm.agg;
+            sm.st_agg[j] = sm.agg[grp];
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(&sm.st_full[j]);
     }
-    if (tid == 0) sm.consumed = consumed;
 }
 
-// Producer warp: claims tiles in ticket order and fills the input ring.
-template <typename T>
+// Producer warp: claims tiles in ticket order and fills the input ring;
+// after the last tile, one end marker per compute group.
+template <typename T, int GRP>
 __device__ __forceinline__ void enc_producer(const EncArgs<T> &a, EncSmem &sm)
 {
     const uint32_t lane = threadIdx.x & 31;
-    uint32_t k = 0;
+    uint32_t k = 0, ends = 0;
     for (;; k++) {
         const int i = (int)(k % kInStages);
         const uint32_t n = k / kInStages;
@@ -1024,7 +1028,7 @@ __device__ __forceinline__ void enc_producer(const EncArgs<T> &a, EncSmem &sm)
         }
         __syncwarp();
         if (lane == 0) enc_issue<T>(a, sm, i, t);  // arrives on in_full after the table
-        if (t >= a.g.ntiles) {
+        if (t >= a.g.ntiles && ++ends == (uint32_t)GRP) {
             k++;
             break;
         }
@@ -1100,38 +1104,41 @@ __device__ __forceinline__ void enc_writer(const EncArgs<T> &a, EncSmem &sm, uin
     }
 }
 
-template <typename T, int VEC, int BINS, bool POOL>
-__global__ void __launch_bounds__(kEncThreads, 1) enc_kernel(const EncArgs<T> a)
+template <typename T, int VEC, int BINS, bool POOL, int GRP, int WPG>
+__global__ void __launch_bounds__(EncShape<GRP, WPG>::kThreads, 1) enc_kernel(const EncArgs<T> a)
 {
+    using S = EncShape<GRP, WPG>;
+    static_assert(GRP <= kMaxGroups, "compute groups");
+    static_assert(kWriters == 1, "end markers are passed to a single writer warp");
     extern __shared__ __align__(128) uint8_t smem_raw[];
     EncSmem &sm = *reinterpret_cast<EncSmem *>(smem_raw);
     const uint32_t tid = threadIdx.x, warp = tid >> 5;
     if (tid == 0) {
         for (int s = 0; s < kInStages; s++) {
             mbar_init(&sm.in_full[s], 1);
-            mbar_init(&sm.in_empty[s], kEncWarps);
+            mbar_init(&sm.in_empty[s], WPG);
         }
         for (int s = 0; s < kStStages; s++) {
-            mbar_init(&sm.st_full[s], kEncWarps);
+            mbar_init(&sm.st_full[s], WPG);
             mbar_init(&sm.st_empty[s], 1);
         }
-        sm.range_err = 0;
-        sm.consumed = 0;
         sm.issued = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    if (warp < (uint32_t)kEncWarps)
-        enc_compute<T, VEC, BINS, POOL>(a, sm);
-    else if (warp == (uint32_t)kProducerWarp)
-        enc_producer<T>(a, sm);
+    if (warp < (uint32_t)S::kCompute)
+        enc_compute<T, VEC, BINS, POOL, GRP, WPG>(a, sm);
+    else if (warp == (uint32_t)S::kProducerWarp)
+        enc_producer<T, GRP>(a, sm);
     else
-        enc_writer<T>(a, sm, warp - (uint32_t)kWriterWarp0);
+        enc_writer<T>(a, sm, warp - (uint32_t)S::kWriterWarp0);
     __syncthreads();
     // After an error a load may still be in flight into a slot nobody
-    // consumed; it must land before the CTA's shared memory is released.
-    if (tid == (uint32_t)kProducerWarp * 32) {
-        for (uint32_t u = sm.consumed; u < sm.issued; u++)
+    // consumed; the last fill of every slot must land before the CTA's
+    // shared memory is released.
+    if (tid == (uint32_t)S::kProducerWarp * 32) {
+        const uint32_t n = sm.issued;
+        for (uint32_t u = n > (uint32_t)kInStages ? n - kInStages : 0; u < n; u++)
             mbar_wait(&sm.in_full[u % kInStages], (u / kInStages) & 1u, a.ctl);
     }
 }
