@@ -43,7 +43,8 @@ typedef enum {
     LSCOMP_ERR_TIMEOUT = 4,  /* a bounded wait inside a kernel ran out */
     LSCOMP_ERR_CORRUPT = 5,  /* stream inconsistent with the given geometry */
     LSCOMP_ERR_RANGE = 6,    /* values the stream format cannot represent */
-    LSCOMP_ERR_NOMEM = 7     /* device or host allocation failed */
+    LSCOMP_ERR_NOMEM = 7,    /* device or host allocation failed */
+    LSCOMP_ERR_TOO_LARGE = 8 /* stack larger than a fixed-size scratch area allows */
 } lscomp_status;
 
 typedef struct lscomp_workspace lscomp_workspace;
@@ -108,6 +109,23 @@ int lscomp_decompress_u32(lscomp_workspace *ws, const uint8_t *d_in, uint64_t cm
 int lscomp_decompress_u32_async(lscomp_workspace *ws, const uint8_t *d_in, uint64_t cmp_len, uint32_t x,
                                 uint32_t y, uint32_t z, const uint32_t bins[4], float pooling,
                                 uint32_t *d_out, void *stream);
+
+/* uint16 compression that allocates nothing (no counterpart in the
+   reference).  For callers that cannot allocate device memory when they
+   compress -- acquisition loops running inside a fixed, pre-reserved memory
+   budget, where a cudaMalloc can fail and synchronises the device, or
+   processes whose device memory belongs to another allocator.  The scan
+   scratch lives in a 2 MiB device array inside the library (per device,
+   held until the process exits), which limits the stack to 262,112 tiles
+   (about 67 million 8x8 blocks); larger stacks return LSCOMP_ERR_TOO_LARGE.
+   Same stream, sizes and synchronisation as lscomp_compress_u16.  All calls
+   on a device share the array: calls that overlap on the GPU race (this
+   function serialises its own calls within a process).  The first call on a
+   device sets up the array's device address; make it before any stream
+   capture. */
+int lscomp_compress_u16_noalloc(const uint16_t *d_in, uint32_t x, uint32_t y, uint32_t z,
+                                const uint32_t bins[4], float pooling, uint8_t *d_out, uint64_t cap,
+                                uint64_t *stream_len, uint64_t *ref_size, void *stream);
 
 /* Wait for the workspace's last launch on `stream` and return its status. */
 int lscomp_workspace_check(lscomp_workspace *ws, void *stream);

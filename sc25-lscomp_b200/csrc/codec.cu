@@ -351,6 +351,7 @@ const char *lscomp_status_string(int s)
     case LSCOMP_ERR_CORRUPT: return "stream inconsistent with the geometry";
     case LSCOMP_ERR_RANGE: return "value range not representable";
     case LSCOMP_ERR_NOMEM: return "out of memory";
+    case LSCOMP_ERR_TOO_LARGE: return "stack too large for the fixed scratch area";
     default: return "unknown status";
     }
 }
@@ -482,3 +483,113 @@ int lscomp_decompress_u32(lscomp_workspace *ws, const uint8_t *d_in, uint64_t cm
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- allocation-free compression
+// lscomp_compress_u16_noalloc: the uint16 encoder with its scan scratch (the
+// launch control block and one look-back word per tile) taken from a
+// file-scope device array instead of a workspace allocation.
+//
+// Who needs it: callers that must not allocate device memory at call time --
+// for example detector acquisition loops that run with a fixed, pre-reserved
+// memory budget (a cudaMalloc there can fail once the budget is used up, and
+// it synchronises the device in the middle of a streaming pipeline), or
+// processes in which another allocator already owns the device memory.  The
+// caller still provides the input and the output buffers; nothing else is
+// allocated: no cudaMalloc, no cudaFree, no library allocator.
+//
+// Limits and sharing: the array is kNoAllocScratchBytes per device, held by
+// every GPU that loads this library until the process exits.  It bounds the
+// stack to kNoAllocMaxTiles tiles (about 67 M 8x8 blocks for 16-bit data);
+// larger stacks are refused with LSCOMP_ERR_TOO_LARGE before any GPU work.
+// All calls on a device share the one array, which keeps the previous call's
+// contents: the control block is cleared on every call (cudaMemsetAsync,
+// which allocates nothing), and the look-back words carry a per-call epoch so
+// stale ones are never mistaken for fresh.  Calls that overlap on the GPU
+// race on the shared array; this function serialises its own calls within a
+// process and returns only after its kernel has finished.  The first call on
+// a device looks up the array's device address (cudaGetSymbolAddress) with
+// that device current; make that first call before any stream capture.
+namespace {
+constexpr size_t kNoAllocScratchBytes = 2u << 20;  // 2 MiB per device
+constexpr size_t kNoAllocCtlBytes = 256;           // LaunchCtl, padded
+constexpr uint64_t kNoAllocMaxTiles = (kNoAllocScratchBytes - kNoAllocCtlBytes) / sizeof(unsigned long long);
+constexpr int kNoAllocMaxDevices = 64;
+static_assert(sizeof(LaunchCtl) <= kNoAllocCtlBytes, "control block fits its slot");
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+struct NoAllocDevice {
+    unsigned char *scratch = nullptr;  // device address of g_noalloc_scratch on this device
+    int sm_count = 0;
+    uint32_t epoch = 0;
+};
+std::mutex g_noalloc_mu;
+NoAllocDevice g_noalloc_dev[kNoAllocMaxDevices];
+}  // namespace
+
+extern "C" int lscomp_compress_u16_noalloc(const uint16_t *d_in, uint32_t x, uint32_t y, uint32_t z,
+                                           const uint32_t bins[4], float pooling, uint8_t *d_out, uint64_t cap,
+                                           uint64_t *stream_len, uint64_t *ref_size, void *stream)
+{
+    if (!d_in || !d_out) return LSCOMP_ERR_ARG;
+    if (reinterpret_cast<uintptr_t>(d_in) % 2u || reinterpret_cast<uintptr_t>(d_out) % 4u) return LSCOMP_ERR_ARG;
+    EncArgs<uint16_t> a;
+    int layout = 0;
+    if (!make_geom(x, y, z, Elem<uint16_t>::kTileBlocks, a.g) || !make_codec(bins, pooling, false, a.c, layout))
+        return LSCOMP_ERR_ARG;
+    if (a.g.ntiles > kNoAllocMaxTiles) return LSCOMP_ERR_TOO_LARGE;
+    if (cap < a.g.R) return LSCOMP_ERR_CAPACITY;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) return LSCOMP_ERR_CUDA;
+    cudaStream_t st = (cudaStream_t)stream;
+
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    NoAllocDevice &d = g_noalloc_dev[dev];
+    if (!d.scratch) {
+        // one-time set-up on this device, with the device current: the host
+        // symbol is only a stand-in, the kernel needs the device address
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_status(e);
+        if (cudaDeviceGetAttribute(&d.sm_count, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            return LSCOMP_ERR_CUDA;
+        d.scratch = static_cast<unsigned char *>(p);
+    }
+    unsigned long long *state = reinterpret_cast<unsigned long long *>(d.scratch + kNoAllocCtlBytes);
+    if (d.epoch >= kEpochMax) {
+        // epochs wrapped: clear the look-back words once
+        cudaError_t e = cudaMemsetAsync(state, 0, kNoAllocMaxTiles * sizeof(unsigned long long), st);
+        if (e != cudaSuccess) return cuda_status(e);
+        d.epoch = 0;
+    }
+    d.epoch++;
+    cudaError_t e = cudaMemsetAsync(d.scratch, 0, sizeof(LaunchCtl), st);
+    if (e != cudaSuccess) return cuda_status(e);
+
+    a.in = d_in;
+    a.out = d_out;
+    a.cap = cap;
+    a.ctl = reinterpret_cast<LaunchCtl *>(d.scratch);
+    a.state = state;
+    a.epoch = d.epoch;
+    a.sizes_out = nullptr;
+    const bool pool = a.c.pool_min <= 64;
+    int s;
+    switch (vec_class(d_in, z, 2)) {
+    case 16: s = launch_enc_v<uint16_t, 16>(a, layout, pool, d.sm_count, st); break;
+    case 4: s = launch_enc_v<uint16_t, 4>(a, layout, pool, d.sm_count, st); break;
+    default: s = launch_enc_v<uint16_t, 2>(a, layout, pool, d.sm_count, st); break;
+    }
+    if (s) return s;
+    LaunchCtl h;  // plain host memory: the copy allocates nothing
+    e = cudaMemcpyAsync(&h, d.scratch, sizeof(LaunchCtl), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_status(e);
+    s = dev_status(h.error);
+    if (s) return s;
+    if (stream_len) *stream_len = h.stream_len;
+    if (ref_size) *ref_size = h.total + a.g.nb;
+    return LSCOMP_OK;
+}

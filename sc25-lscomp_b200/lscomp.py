@@ -37,6 +37,7 @@ STATUS = {
     5: "stream inconsistent with the geometry",
     6: "value range not representable",
     7: "out of memory",
+    8: "stack too large for the fixed scratch area",
 }
 
 
