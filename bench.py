@@ -284,7 +284,7 @@ def main():
             pass
     value = world * 4 * nbytes / (ms_step / 1e3) / 1e9
 
-    e2e = bench_e2e(args, dims, ws, h, dev, nbytes, sizes, world)
+    e2e = bench_e2e(args, dims, ws, h, dev, nbytes, sizes, world) if args.e2e_steps > 0 else None
     out = {"metric": "lsCOMP compress+decompress throughput (lossless and lossy b=3 5 10 15 p=0.5), "
                      "uncompressed GB per second",
            "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
