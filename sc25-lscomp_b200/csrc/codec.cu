@@ -64,6 +64,14 @@ int pool_min_zeros(float p)
     return 65;
 }
 
+// ceil(2^64 / b) for b >= 2: with 2^64 - 1 = q b + r (0 <= r < b), 2^64 / b
+// = q + (r + 1) / b and 0 < r + 1 <= b, so the ceiling is always q + 1
+unsigned long long magic64(uint32_t b)
+{
+    if (b < 2) return 0;
+    return ~0ull / b + 1;
+}
+
 bool make_geom(uint32_t X, uint32_t Y, uint32_t Z, uint32_t tile_blocks, Geom &g)
 {
     if (!X || !Y || !Z) return false;
@@ -89,15 +97,9 @@ bool make_geom(uint32_t X, uint32_t Y, uint32_t Z, uint32_t tile_blocks, Geom &g
         g.ntiles = g.nrows_b * g.nc;
         g.inv_bzb = 0;
     }
+    g.byb_magic = magic64(g.byb);
+    g.nc_magic = magic64(g.nc);
     return true;
-}
-
-// ceil(2^64 / b) for b >= 2: with 2^64 - 1 = q b + r (0 <= r < b), 2^64 / b
-// = q + (r + 1) / b and 0 < r + 1 <= b, so the ceiling is always q + 1
-unsigned long long magic64(uint32_t b)
-{
-    if (b < 2) return 0;
-    return ~0ull / b + 1;
 }
 
 bool make_codec(const uint32_t bins[4], float p, bool wide, Codec &c, int &layout)

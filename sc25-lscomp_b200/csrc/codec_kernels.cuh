@@ -104,6 +104,7 @@ struct Geom {
     uint32_t G;                // block-rows per tile (whole-row tiles)
     uint32_t nc, W;            // chunks per block-row, chunk width (chunked tiles)
     uint32_t inv_bzb;          // ceil(65536 / bzb), exact b / bzb for b < 256 (whole-row tiles)
+    unsigned long long byb_magic, nc_magic;  // ceil(2^64 / d) of byb and nc (0 for d = 1)
 };
 
 struct Codec {
@@ -149,6 +150,16 @@ struct TileInfo {
     uint32_t c0;             // first block column (chunked tiles)
 };
 
+// n / d from m = ceil(2^64 / d) (m = 0 for d = 1): the high product is
+// exact while n d < 2^64 and at most one too large past that
+__device__ __forceinline__ unsigned long long udiv_magic(unsigned long long n, uint32_t d, unsigned long long m)
+{
+    if (m == 0) return n;
+    unsigned long long q = __umul64hi(n, m);
+    if (q * d > n) q--;
+    return q;
+}
+
 __device__ __forceinline__ TileInfo tile_info(const Geom &g, unsigned long long t)
 {
     TileInfo ti;
@@ -160,7 +171,7 @@ __device__ __forceinline__ TileInfo tile_info(const Geom &g, unsigned long long 
         ti.k0 = ti.rho0 * g.bzb;
         ti.c0 = 0;
     } else {
-        ti.rho0 = t / g.nc;
+        ti.rho0 = udiv_magic(t, g.nc, g.nc_magic);
         uint32_t ci = (uint32_t)(t - ti.rho0 * g.nc);
         ti.c0 = ci * g.W;
         uint32_t c1 = ti.c0 + g.W;
@@ -175,7 +186,7 @@ __device__ __forceinline__ TileInfo tile_info(const Geom &g, unsigned long long 
 // first image row (frame-major global row index) and row count of a block-row
 __device__ __forceinline__ unsigned long long brow_start(const Geom &g, unsigned long long rho, uint32_t &nrows)
 {
-    unsigned long long x = rho / g.byb;
+    unsigned long long x = udiv_magic(rho, g.byb, g.byb_magic);
     uint32_t by = (uint32_t)(rho - x * g.byb);
     uint32_t r = g.Y - 8u * by;
     nrows = r < 8u ? r : 8u;
@@ -617,12 +628,12 @@ __device__ __forceinline__ unsigned long long tile_prefix(unsigned long long *st
     const uint32_t lane = threadIdx.x & 31;
     ok = true;
     if (tile == 0) {
-        if (lane == 0) st_release_u64(state, make_state(epoch, kFlagIncl, agg));
+        if (lane == 0) st_relaxed_u64(state, make_state(epoch, kFlagIncl, agg));
         return 0;
     }
-    if (lane == 0) st_release_u64(state + tile, make_state(epoch, kFlagAgg, agg));
+    if (lane == 0) st_relaxed_u64(state + tile, make_state(epoch, kFlagAgg, agg));
     unsigned long long excl = lookback_warp(state, tile, epoch, ctl, ok);
-    if (ok && lane == 0) st_release_u64(state + tile, make_state(epoch, kFlagIncl, excl + agg));
+    if (ok && lane == 0) st_relaxed_u64(state + tile, make_state(epoch, kFlagIncl, excl + agg));
     return excl;
 }
 
@@ -964,7 +975,7 @@ __device__ __forceinline__ void enc_compute(const EncArgs<T> &a, EncSmem &sm)
             const uint32_t agg = tile_scan(hdr, off, ti.nblk);
             if (lane == 0) {
                 sm.agg[grp] = agg;
-                st_release_u64(a.state + t, make_state(a.epoch, t == 0 ? kFlagIncl : kFlagAgg, agg));
+                st_relaxed_u64(a.state + t, make_state(a.epoch, t == 0 ? kFlagIncl : kFlagAgg, agg));
             }
         }
         for (uint32_t b = gtid; b < ti.nblk; b += WPG * 32) a.out[ti.k0 + b] = hdr[b];
@@ -1001,14 +1012,19 @@ __device__ __forceinline__ void enc_producer(const EncArgs<T> &a, EncSmem &sm)
 {
     const uint32_t lane = threadIdx.x & 31;
     uint32_t k = 0, ends = 0;
+    unsigned long long next = 0;  // the next tile, claimed one tile ahead
+    if (lane == 0) next = atomicAdd(&a.ctl->ticket, 1ull);
     for (;; k++) {
         const int i = (int)(k % kInStages);
         const uint32_t n = k / kInStages;
         bool ok = mbar_wait(&sm.in_empty[i], (n & 1u) ^ 1u, a.ctl);
         if (!__all_sync(0xffffffffu, ok)) break;
-        unsigned long long t = 0;
-        if (lane == 0) t = aborted(a.ctl) ? a.g.ntiles : atomicAdd(&a.ctl->ticket, 1ull);
-        t = __shfl_sync(0xffffffffu, t, 0);
+        unsigned long long t = __shfl_sync(0xffffffffu, next, 0);
+        if (t < a.g.ntiles) {
+            if (lane == 0) next = atomicAdd(&a.ctl->ticket, 1ull);
+        } else {
+            t = a.g.ntiles;
+        }
         if (t < a.g.ntiles) {
             // block-row table of the tile for the compute warps
             const Geom &g = a.g;
@@ -1064,7 +1080,7 @@ __device__ __forceinline__ void enc_writer(const EncArgs<T> &a, EncSmem &sm, uin
             excl = lookback_warp(a.state, t, a.epoch, a.ctl, lok);
 #endif
             if (!lok) break;
-            if (lane == 0) st_release_u64(a.state + t, make_state(a.epoch, kFlagIncl, excl + agg));
+            if (lane == 0) st_relaxed_u64(a.state + t, make_state(a.epoch, kFlagIncl, excl + agg));
         }
         floor = (long long)t;
         floor_incl = excl + agg;

@@ -24,7 +24,7 @@ enum DevError : uint32_t {
 // Per-launch control block in device memory.  Zeroed by the host (one
 // cudaMemsetAsync) before every launch.
 struct LaunchCtl {
-    unsigned long long ticket;   // next tile to claim
+    unsigned long long ticket;   // next tile to claim (pushed past every tile on abort)
     unsigned int error;          // first DevError seen
     unsigned int abort;          // set with error: every CTA stops waiting
     unsigned long long total;    // payload bytes of the stream (encoder)
@@ -33,6 +33,7 @@ struct LaunchCtl {
 };
 
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s for any single wait
+constexpr unsigned long long kTicketAbort = 1ull << 48;     // added to the ticket on abort
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p)
 {
@@ -50,6 +51,7 @@ __device__ __forceinline__ void raise_error(LaunchCtl *ctl, uint32_t code)
 {
     atomicCAS(&ctl->error, 0u, code);
     atomicExch(&ctl->abort, 1u);
+    atomicAdd(&ctl->ticket, kTicketAbort);  // every later claim is past the end
 }
 
 __device__ __forceinline__ bool aborted(const LaunchCtl *ctl)
@@ -79,15 +81,19 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t by
                  : "memory");
 }
 
+// A waiting thread is suspended until the phase completes (or this many
+// nanoseconds pass), so waiting warps take no issue slots from working ones.
+constexpr uint32_t kSuspendHintNs = 1000000u;
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
 {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(ok)
-        : "r"(smem_addr(bar)), "r"(parity)
+        : "r"(smem_addr(bar)), "r"(parity), "r"(kSuspendHintNs)
         : "memory");
     return ok != 0;
 }
@@ -132,15 +138,18 @@ __device__ __forceinline__ void fence_proxy_async_smem()
 }
 
 // ---------------------------------------------------------------- gpu scope
-__device__ __forceinline__ void st_release_u64(unsigned long long *p, unsigned long long v)
+// The look-back state words carry their flag and value in one 64-bit word
+// and nothing else is read on the strength of them, so relaxed gpu-scope
+// accesses suffice (no fence before a publication).
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long *p, unsigned long long v)
 {
-    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
-__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p)
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long *p)
 {
     unsigned long long v;
-    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
     return v;
 }
 
@@ -181,7 +190,7 @@ __device__ __forceinline__ unsigned long long lookback_warp(const unsigned long 
         uint32_t flag;
         unsigned long long val;
         if (idx >= 0) {
-            unsigned long long w = ld_acquire_u64(state + idx);
+            unsigned long long w = ld_relaxed_u64(state + idx);
             bool fresh = (uint32_t)(w >> kEpochShift) == epoch;
             flag = fresh ? (uint32_t)((w >> kFlagShift) & 3u) : 0u;
             val = w & kValueMask;
@@ -219,12 +228,6 @@ __device__ __forceinline__ unsigned long long lookback_warp(const unsigned long 
     return excl;
 }
 
-__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long *p)
-{
-    unsigned long long v;
-    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-    return v;
-}
 
 // Decoupled look-back with a known floor: the exclusive prefix of `tile`
 // from the state words of tiles floor+1 .. tile-1 plus the inclusive prefix
