@@ -561,7 +561,7 @@ constexpr int kMaxGroups = 2;
 struct EncSmem {
     alignas(128) uint8_t in[kInStages][kStageBytes];
     alignas(128) uint8_t st[kStStages][kStagingBytes];
-    uint64_t in_full[kInStages];       // producer -> compute: tile input landed
+    uint64_t in_full[kInStages];       // producer -> compute: input of entries k = s mod 2 kInStages landed
     uint64_t in_empty[kInStages];      // compute -> producer: input slot read
     uint64_t st_full[kStStages];       // compute -> writer: payload packed
     uint64_t st_empty[kStStages];      // writer -> compute: payload written out
@@ -578,7 +578,23 @@ struct EncSmem {
     uint32_t off[kMaxGroups][kMaxTileBlocks];  // payload offset of each block inside the tile
     uint32_t agg[kMaxGroups];
     uint32_t issued;                           // input-ring entries the producer filled
+    // input landed, entries k = kInStages + s mod 2 kInStages.  With one
+    // barrier per entry mod 2 kInStages a group waiting for entry k cannot
+    // pass on the still-pending phase of entry k - kInStages (the other
+    // group's tile in the same slot, whose load may land after the group's
+    // previous one): the phase before entry k's belongs to the group's own
+    // entry k - 2 kInStages, which it has already consumed.
+    uint64_t in_full2[kInStages];
 };
+
+// The landing barrier of ring entry k and the parity of its phase.
+__device__ __forceinline__ uint64_t *entry_full(EncSmem &sm, uint32_t k)
+{
+    const uint32_t s = k % kInStages;
+    return ((k / kInStages) & 1u) ? &sm.in_full2[s] : &sm.in_full[s];
+}
+
+__device__ __forceinline__ uint32_t entry_parity(uint32_t k) { return (k / (2 * kInStages)) & 1u; }
 
 struct DecSmem {
     uint32_t br_rel[kMaxTileBlocks];
@@ -640,11 +656,11 @@ __device__ __forceinline__ unsigned long long tile_prefix(unsigned long long *st
 // ---------------------------------------------------------------- encoder
 // Thread 0: claim-time bookkeeping and TMA issue for one tile into stage s.
 template <typename T>
-__device__ void enc_issue(const EncArgs<T> &a, EncSmem &sm, int s, unsigned long long t)
+__device__ void enc_issue(const EncArgs<T> &a, EncSmem &sm, int s, unsigned long long t, uint64_t *full)
 {
     sm.in_tile[s] = t;
     if (t >= a.g.ntiles) {
-        mbar_arrive(&sm.in_full[s]);
+        mbar_arrive(full);
         return;
     }
     constexpr uint32_t ES = sizeof(T);
@@ -699,10 +715,10 @@ __device__ void enc_issue(const EncArgs<T> &a, EncSmem &sm, int s, unsigned long
             *reinterpret_cast<T *>(sb + (p - gs)) = *reinterpret_cast<const T *>(p);
     }
     fence_proxy_async_smem();
-    mbar_arrive_expect_tx(&sm.in_full[s], tx);
+    mbar_arrive_expect_tx(full, tx);
     for (uint32_t i = 0; i < nr; i++)
         if (ce_[i] > cs_[i])
-            bulk_g2s(dst_[i], reinterpret_cast<const void *>(cs_[i]), (uint32_t)(ce_[i] - cs_[i]), &sm.in_full[s]);
+            bulk_g2s(dst_[i], reinterpret_cast<const void *>(cs_[i]), (uint32_t)(ce_[i] - cs_[i]), full);
 }
 
 // Where a lane's two row segments (rows r and r+4 of tile-local block b)
@@ -924,8 +940,8 @@ __device__ __forceinline__ void enc_compute(const EncArgs<T> &a, EncSmem &sm)
     uint32_t *const off = sm.off[grp];
     for (uint32_t k = grp;; k += GRP) {
         const int i = (int)(k % kInStages), j = (int)(k % kStStages);
-        const uint32_t n = k / kInStages, m = k / kStStages;
-        bool ok = mbar_wait(&sm.in_full[i], n & 1u, a.ctl);
+        const uint32_t m = k / kStStages;
+        bool ok = mbar_wait(entry_full(sm, k), entry_parity(k), a.ctl);
         if (!group_bar_and(barid, WPG * 32, ok)) break;
         const unsigned long long t = sm.in_tile[i];
         if (t >= g.ntiles) {
@@ -1043,7 +1059,7 @@ __device__ __forceinline__ void enc_producer(const EncArgs<T> &a, EncSmem &sm)
             }
         }
         __syncwarp();
-        if (lane == 0) enc_issue<T>(a, sm, i, t);  // arrives on in_full after the table
+        if (lane == 0) enc_issue<T>(a, sm, i, t, entry_full(sm, k));  // after the table
         if (t >= a.g.ntiles && ++ends == (uint32_t)GRP) {
             k++;
             break;
@@ -1132,6 +1148,7 @@ __global__ void __launch_bounds__(EncShape<GRP, WPG>::kThreads, 1) enc_kernel(co
     if (tid == 0) {
         for (int s = 0; s < kInStages; s++) {
             mbar_init(&sm.in_full[s], 1);
+            mbar_init(&sm.in_full2[s], 1);
             mbar_init(&sm.in_empty[s], WPG);
         }
         for (int s = 0; s < kStStages; s++) {
@@ -1155,7 +1172,7 @@ __global__ void __launch_bounds__(EncShape<GRP, WPG>::kThreads, 1) enc_kernel(co
     if (tid == (uint32_t)S::kProducerWarp * 32) {
         const uint32_t n = sm.issued;
         for (uint32_t u = n > (uint32_t)kInStages ? n - kInStages : 0; u < n; u++)
-            mbar_wait(&sm.in_full[u % kInStages], (u / kInStages) & 1u, a.ctl);
+            mbar_wait(entry_full(sm, u), entry_parity(u), a.ctl);
     }
 }
 
