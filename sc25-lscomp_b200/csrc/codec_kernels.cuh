@@ -654,59 +654,77 @@ __device__ __forceinline__ unsigned long long tile_prefix(unsigned long long *st
 }
 
 // ---------------------------------------------------------------- encoder
-// Thread 0: claim-time bookkeeping and TMA issue for one tile into stage s.
+// Producer warp, all lanes: the block-row table, range bookkeeping and TMA
+// issue of tile t into input slot s; the copies complete on `full`.  The
+// block-row starts of the tile are computed one per lane, so the warp's
+// dependent chain is that of a single block-row.
 template <typename T>
-__device__ void enc_issue(const EncArgs<T> &a, EncSmem &sm, int s, unsigned long long t, uint64_t *full)
+__device__ void enc_issue(const EncArgs<T> &a, EncSmem &sm, int s, unsigned long long t, uint64_t *full,
+                          uint32_t lane)
 {
-    sm.in_tile[s] = t;
-    if (t >= a.g.ntiles) {
-        mbar_arrive(full);
+    const Geom &g = a.g;
+    if (t >= g.ntiles) {
+        if (lane == 0) {
+            sm.in_tile[s] = t;
+            mbar_arrive(full);
+        }
         return;
     }
     constexpr uint32_t ES = sizeof(T);
-    const Geom &g = a.g;
-    TileInfo ti = tile_info(g, t);
-    const uintptr_t base = reinterpret_cast<uintptr_t>(a.in);
-    const uintptr_t A0 = (base + 15) & ~(uintptr_t)15;
-    const uintptr_t A1 = (base + ES * g.N) & ~(uintptr_t)15;
-    uint8_t *stage = sm.in[s];
-
-    // ranges: whole-row tiles -> 1 contiguous range; chunked -> one per row
+    const TileInfo ti = tile_info(g, t);
+    // ranges: whole-row tiles -> 1 contiguous range; chunked -> one per row.
+    // Lane r < nr holds range r: first element es, element count ne.
     uint32_t nr;
-    unsigned long long es[8], ne[8];
+    unsigned long long es = 0, ne = 0;
     if (!g.chunked) {
-        uint32_t rows_first, rows_last;
-        unsigned long long r0 = brow_start(g, ti.rho0, rows_first);
-        unsigned long long rl = brow_start(g, ti.rho0 + ti.nbr - 1, rows_last);
-        es[0] = r0 * g.Z;
-        ne[0] = (rl + rows_last) * g.Z - es[0];
+        unsigned long long r0 = 0, rend = 0;
+        for (uint32_t q0 = 0; q0 <= ti.nbr; q0 += 32) {
+            const uint32_t q = q0 + lane;
+            uint32_t nrows = 0;
+            unsigned long long rs = 0;
+            if (q <= ti.nbr) {
+                const unsigned long long rho = ti.rho0 + q;
+                rs = rho < g.nrows_b ? brow_start(g, rho, nrows) : (unsigned long long)g.X * g.Y;
+            }
+            if (q0 == 0) r0 = __shfl_sync(0xffffffffu, rs, 0);
+            if (q < ti.nbr) {
+                sm.br_rel[s][q] = (uint32_t)((rs - r0) * g.Z);
+                sm.br_rows[s][q] = (uint8_t)nrows;
+            }
+            const uint32_t last = ti.nbr - q0;  // lane holding the end row in this pass
+            if (last < 32u) rend = __shfl_sync(0xffffffffu, rs, last);
+        }
         nr = 1;
+        es = r0 * g.Z;
+        ne = (rend - r0) * g.Z;
     } else {
         uint32_t rows;
-        unsigned long long r0 = brow_start(g, ti.rho0, rows);
-        uint32_t col0 = 8u * ti.c0;
+        const unsigned long long r0 = brow_start(g, ti.rho0, rows);
+        if (lane == 0) sm.br_rows[s][0] = (uint8_t)rows;
+        const uint32_t col0 = 8u * ti.c0;
         uint32_t col1 = 8u * (ti.c0 + ti.nblk);
         if (col1 > g.Z) col1 = g.Z;
         nr = rows;
-        for (uint32_t r = 0; r < rows; r++) {
-            es[r] = (r0 + r) * g.Z + col0;
-            ne[r] = col1 - col0;
-        }
+        es = (r0 + lane) * g.Z + col0;
+        ne = col1 - col0;
     }
+    const uintptr_t base = reinterpret_cast<uintptr_t>(a.in);
+    const uintptr_t A0 = (base + 15) & ~(uintptr_t)15;
+    const uintptr_t A1 = (base + ES * g.N) & ~(uintptr_t)15;
     uint32_t tx = 0;
-    uintptr_t cs_[8], ce_[8];
-    uint8_t *dst_[8];
-    for (uint32_t i = 0; i < nr; i++) {
-        uint8_t *sb = stage + (g.chunked ? i * kChunkPitch : 0);
-        uintptr_t ga = base + ES * es[i];
-        uintptr_t ge = ga + ES * ne[i];
-        uintptr_t gs = ga & ~(uintptr_t)15;
-        sm.in_mis[s][i] = (uint32_t)(ga & 15);
-        uintptr_t cs = gs > A0 ? gs : A0;
-        uintptr_t ce = (ge + 15) & ~(uintptr_t)15;
+    uintptr_t cs = 0, ce = 0;
+    uint8_t *dst = nullptr;
+    if (lane < nr) {
+        uint8_t *sb = sm.in[s] + (g.chunked ? lane * kChunkPitch : 0u);
+        const uintptr_t ga = base + ES * es;
+        const uintptr_t ge = ga + ES * ne;
+        const uintptr_t gs = ga & ~(uintptr_t)15;
+        sm.in_mis[s][lane] = (uint32_t)(ga & 15);
+        cs = gs > A0 ? gs : A0;
+        ce = (ge + 15) & ~(uintptr_t)15;
         if (ce > A1) ce = A1;
-        cs_[i] = cs; ce_[i] = ce; dst_[i] = sb + (cs - gs);
-        if (ce > cs) tx += (uint32_t)(ce - cs);
+        dst = sb + (cs - gs);
+        if (ce > cs) tx = (uint32_t)(ce - cs);
         // bytes outside the 16-byte-aligned interior of the whole array
         // (only the first and last tiles): copy them element by element
         for (uintptr_t p = ga; p < ge && p < A0; p += ES)
@@ -714,11 +732,13 @@ __device__ void enc_issue(const EncArgs<T> &a, EncSmem &sm, int s, unsigned long
         for (uintptr_t p = (ga > A1 ? ga : A1); p < ge; p += ES)
             *reinterpret_cast<T *>(sb + (p - gs)) = *reinterpret_cast<const T *>(p);
     }
+    if (lane == 0) sm.in_tile[s] = t;
     fence_proxy_async_smem();
-    mbar_arrive_expect_tx(full, tx);
-    for (uint32_t i = 0; i < nr; i++)
-        if (ce_[i] > cs_[i])
-            bulk_g2s(dst_[i], reinterpret_cast<const void *>(cs_[i]), (uint32_t)(ce_[i] - cs_[i]), full);
+    tx = __reduce_add_sync(0xffffffffu, tx);
+    __syncwarp();
+    if (lane == 0) mbar_arrive_expect_tx(full, tx);
+    __syncwarp();
+    if (lane < nr && ce > cs) bulk_g2s(dst, reinterpret_cast<const void *>(cs), (uint32_t)(ce - cs), full);
 }
 
 // Where a lane's two row segments (rows r and r+4 of tile-local block b)
@@ -1041,25 +1061,8 @@ __device__ __forceinline__ void enc_producer(const EncArgs<T> &a, EncSmem &sm)
         } else {
             t = a.g.ntiles;
         }
-        if (t < a.g.ntiles) {
-            // block-row table of the tile for the compute warps
-            const Geom &g = a.g;
-            const TileInfo ti = tile_info(g, t);
-            uint32_t n0;
-            const unsigned long long r0 = brow_start(g, ti.rho0, n0);
-            if (!g.chunked) {
-                for (uint32_t q = lane; q < ti.nbr; q += 32) {
-                    uint32_t nrows;
-                    const unsigned long long rs = brow_start(g, ti.rho0 + q, nrows);
-                    sm.br_rel[i][q] = (uint32_t)((rs - r0) * g.Z);
-                    sm.br_rows[i][q] = (uint8_t)nrows;
-                }
-            } else if (lane == 0) {
-                sm.br_rows[i][0] = (uint8_t)n0;
-            }
-        }
         __syncwarp();
-        if (lane == 0) enc_issue<T>(a, sm, i, t, entry_full(sm, k));  // after the table
+        enc_issue<T>(a, sm, i, t, entry_full(sm, k), lane);  // the whole warp
         if (t >= a.g.ntiles && ++ends == (uint32_t)GRP) {
             k++;
             break;
