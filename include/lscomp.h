@@ -127,6 +127,32 @@ int lscomp_compress_u16_noalloc(const uint16_t *d_in, uint32_t x, uint32_t y, ui
                                 const uint32_t bins[4], float pooling, uint8_t *d_out, uint64_t cap,
                                 uint64_t *stream_len, uint64_t *ref_size, void *stream);
 
+/* Batch compression (no counterpart in the reference, whose host API takes
+   one stack per call).  n stacks of any shapes, all with the same bins and
+   pooling threshold, compressed by one persistent launch: the tiles of all
+   stacks share the GPU, so many small stacks (a few frames each) cost about
+   what one stack of their total size costs, instead of one launch and one
+   host round trip each.  Each stack's stream is exactly the stream
+   lscomp_compress_u16 / _u32 writes for that stack alone; stream_len[i] and
+   ref_size[i] (host arrays of n entries, either may be NULL) receive its
+   length and the reference-reported size.  The stacks' input and output
+   buffers must not overlap.  Synchronises the stream.  Allocates (once per
+   workspace, when a batch is larger than any before) about 120 bytes per
+   stack and 4 bytes per tile of device memory, plus pinned staging. */
+typedef struct lscomp_stack {
+    const void *d_in; /* X*Y*Z elements of the call's type (uint16 or uint32) */
+    uint32_t x, y, z; /* dims, z fastest */
+    uint8_t *d_out;   /* stream buffer, 4-byte aligned */
+    uint64_t cap;     /* its capacity in bytes (lscomp_max_stream_bytes_* is always enough) */
+} lscomp_stack;
+
+int lscomp_compress_batch_u16(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n,
+                              const uint32_t bins[4], float pooling, uint64_t *stream_len,
+                              uint64_t *ref_size, void *stream);
+int lscomp_compress_batch_u32(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n,
+                              const uint32_t bins[4], float pooling, uint64_t *stream_len,
+                              uint64_t *ref_size, void *stream);
+
 /* Wait for the workspace's last launch on `stream` and return its status. */
 int lscomp_workspace_check(lscomp_workspace *ws, void *stream);
 

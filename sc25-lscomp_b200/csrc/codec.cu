@@ -9,234 +9,14 @@
 #include <atomic>
 #include <mutex>
 #include "lscomp.h"
-#include "codec_kernels.cuh"
+#include "codec_host.h"
 
 using namespace lsc;
 
-namespace {
-
-std::atomic<uint64_t> g_launches{0};
-
-constexpr uint32_t kEpochMax = (1u << 20) - 1;
-
-}  // namespace
-
-struct lscomp_workspace {
-    int device = 0;
-    int sm_count = 0;
-    LaunchCtl *ctl = nullptr;          // device
-    LaunchCtl *h_ctl = nullptr;        // pinned host mirror for status reads
-    unsigned long long *state = nullptr;   // look-back words, then per-tile offsets
-    uint64_t state_cap = 0;            // entries of each of the two arrays
-    uint32_t epoch = 0;
-    std::mutex mu;
-};
+using namespace lsc_host;
 
 namespace {
 
-int cuda_status(cudaError_t e)
-{
-    if (e == cudaSuccess) return LSCOMP_OK;
-    if (e == cudaErrorMemoryAllocation) return LSCOMP_ERR_NOMEM;
-    return LSCOMP_ERR_CUDA;
-}
-
-int dev_status(uint32_t e)
-{
-    switch (e) {
-    case DEV_OK: return LSCOMP_OK;
-    case DEV_ERR_TIMEOUT: return LSCOMP_ERR_TIMEOUT;
-    case DEV_ERR_CAPACITY: return LSCOMP_ERR_CAPACITY;
-    case DEV_ERR_CORRUPT: return LSCOMP_ERR_CORRUPT;
-    case DEV_ERR_RANGE: return LSCOMP_ERR_RANGE;
-    default: return LSCOMP_ERR_CUDA;
-    }
-}
-
-// smallest zero count k (0..64) with (float)k/64 > p, 65 if none
-// (lsCOMP/src/cuLSZ_kernel.cu:920-921; k/64 is exact in binary32)
-int pool_min_zeros(float p)
-{
-    for (int k = 0; k <= 64; k++) {
-        float sparsity = (float)k / 64.0f;
-        if (sparsity > p) return k;
-    }
-    return 65;
-}
-
-// ceil(2^64 / b) for b >= 2: with 2^64 - 1 = q b + r (0 <= r < b), 2^64 / b
-// = q + (r + 1) / b and 0 < r + 1 <= b, so the ceiling is always q + 1
-unsigned long long magic64(uint32_t b)
-{
-    if (b < 2) return 0;
-    return ~0ull / b + 1;
-}
-
-bool make_geom(uint32_t X, uint32_t Y, uint32_t Z, uint32_t tile_blocks, Geom &g)
-{
-    if (!X || !Y || !Z) return false;
-    g.X = X; g.Y = Y; g.Z = Z;
-    g.byb = (Y + 7) / 8;
-    g.bzb = (Z + 7) / 8;
-    g.nrows_b = (unsigned long long)X * g.byb;
-    g.nb = g.nrows_b * g.bzb;
-    g.R = (g.nb + 3) / 4 * 4;
-    g.N = (unsigned long long)X * Y * Z;
-    if (g.bzb <= tile_blocks) {
-        g.chunked = 0;
-        g.G = tile_blocks / g.bzb;
-        g.ntiles = (g.nrows_b + g.G - 1) / g.G;
-        g.nc = 1;
-        g.W = g.bzb;
-        g.inv_bzb = (65536u + g.bzb - 1) / g.bzb;
-    } else {
-        g.chunked = 1;
-        g.G = 1;
-        g.nc = (g.bzb + tile_blocks - 1) / tile_blocks;
-        g.W = (g.bzb + g.nc - 1) / g.nc;
-        g.ntiles = g.nrows_b * g.nc;
-        g.inv_bzb = 0;
-    }
-    g.byb_magic = magic64(g.byb);
-    g.nc_magic = magic64(g.nc);
-    return true;
-}
-
-bool make_codec(const uint32_t bins[4], float p, bool wide, Codec &c, int &layout)
-{
-    if (!bins) return false;
-    for (int k = 0; k < 4; k++) {
-        if (bins[k] == 0) return false;
-        c.bins[k] = bins[k];
-        c.magic[k] = bins[k] == 1 ? 0u : (uint32_t)((0x100000000ull + bins[k] - 1) / bins[k]);
-        c.magic64[k] = magic64(bins[k]);
-        c.binc[k] = (!wide && bins[k] > 65536u) ? 65536u : bins[k];
-    }
-    c.pool_min = pool_min_zeros(p);
-    if (bins[0] == 1 && bins[1] == 1 && bins[2] == 1 && bins[3] == 1)
-        layout = BINS_IDENT;
-    else if (bins[0] == bins[1] && bins[1] == bins[2] && bins[2] == bins[3])
-        layout = BINS_EQUAL;
-    else if (bins[0] <= bins[1] && bins[1] <= bins[2] && bins[2] <= bins[3])
-        layout = BINS_MONO;
-    else
-        layout = BINS_GENERAL;
-    return true;
-}
-
-// widest access every row segment of the stack allows (bytes)
-int vec_class(const void *p, uint32_t Z, size_t es)
-{
-    uintptr_t a = reinterpret_cast<uintptr_t>(p);
-    if (es == 2) {
-        if ((Z % 8u) == 0 && (a % 16u) == 0) return 16;
-        if ((Z % 2u) == 0 && (a % 4u) == 0) return 4;
-        return 2;
-    }
-    if ((Z % 4u) == 0 && (a % 16u) == 0) return 16;
-    return 4;
-}
-
-// Ensure the workspace holds `ntiles` scan slots and hand out a fresh epoch.
-int ws_prepare(lscomp_workspace *ws, uint64_t ntiles, cudaStream_t st)
-{
-    if (ntiles > ws->state_cap) {
-        uint64_t cap = ntiles + ntiles / 4 + 1024;
-        unsigned long long *p = nullptr;
-        cudaError_t e = cudaStreamSynchronize(st);
-        if (e != cudaSuccess) return cuda_status(e);
-        if (ws->state) cudaFree(ws->state);
-        ws->state = nullptr;
-        ws->state_cap = 0;
-        e = cudaMalloc(&p, 2 * cap * sizeof(unsigned long long));
-        if (e != cudaSuccess) return cuda_status(e);
-        e = cudaMemsetAsync(p, 0, 2 * cap * sizeof(unsigned long long), st);
-        if (e != cudaSuccess) { cudaFree(p); return cuda_status(e); }
-        ws->state = p;
-        ws->state_cap = cap;
-        ws->epoch = 0;
-    }
-    if (ws->epoch >= kEpochMax) {
-        cudaError_t e = cudaMemsetAsync(ws->state, 0, ws->state_cap * sizeof(unsigned long long), st);
-        if (e != cudaSuccess) return cuda_status(e);
-        ws->epoch = 0;
-    }
-    ws->epoch++;
-    cudaError_t e = cudaMemsetAsync(ws->ctl, 0, sizeof(LaunchCtl), st);
-    return cuda_status(e);
-}
-
-template <typename K>
-int ctas_per_sm(K kernel, size_t smem)
-{
-    int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, kThreads, smem) != cudaSuccess) return 1;
-    return n > 0 ? n : 1;
-}
-
-template <typename T, int VEC, int BINS, bool POOL, int GRP, int WPG>
-int launch_enc_w(const EncArgs<T> &a, int sm_count, cudaStream_t st)
-{
-    auto k = enc_kernel<T, VEC, BINS, POOL, GRP, WPG>;
-    const size_t smem = sizeof(EncSmem);
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    // persistent: one CTA per SM (the CTA holds ~200 KB of rings)
-    unsigned long long grid = (unsigned long long)sm_count;
-    if (grid > a.g.ntiles) grid = a.g.ntiles;
-    k<<<(unsigned)grid, EncShape<GRP, WPG>::kThreads, smem, st>>>(a);
-    g_launches.fetch_add(1);
-    return cuda_status(cudaGetLastError());
-}
-
-// Compute warps per encoder CTA: LSC_ENC_GROUPS groups of LSC_ENC_WPG warps.
-template <typename T, int VEC, int BINS, bool POOL>
-int launch_enc_t(const EncArgs<T> &a, int sm_count, cudaStream_t st)
-{
-    return launch_enc_w<T, VEC, BINS, POOL, LSC_ENC_GROUPS, LSC_ENC_WPG>(a, sm_count, st);
-}
-
-template <typename T, int VEC>
-int launch_enc_v(const EncArgs<T> &a, int layout, bool pool, int sm, cudaStream_t st)
-{
-    if (layout == BINS_IDENT)
-        return pool ? launch_enc_t<T, VEC, BINS_IDENT, true>(a, sm, st)
-                    : launch_enc_t<T, VEC, BINS_IDENT, false>(a, sm, st);
-    if (layout == BINS_EQUAL)
-        return pool ? launch_enc_t<T, VEC, BINS_EQUAL, true>(a, sm, st)
-                    : launch_enc_t<T, VEC, BINS_EQUAL, false>(a, sm, st);
-    if (layout == BINS_MONO)
-        return pool ? launch_enc_t<T, VEC, BINS_MONO, true>(a, sm, st)
-                    : launch_enc_t<T, VEC, BINS_MONO, false>(a, sm, st);
-    return pool ? launch_enc_t<T, VEC, BINS_GENERAL, true>(a, sm, st)
-                : launch_enc_t<T, VEC, BINS_GENERAL, false>(a, sm, st);
-}
-
-template <typename T, int VEC>
-int launch_dec_t(const DecArgs<T> &a, int sm_count, cudaStream_t st)
-{
-    // 1) per-tile stream offsets from the header bytes
-    const unsigned long long nseg = (a.g.ntiles + kSegTiles - 1) / kSegTiles;
-    unsigned long long grid = (unsigned long long)sm_count * 4;
-    if (grid > nseg) grid = nseg;
-    dec_offsets_kernel<T><<<(unsigned)grid, kThreads, 0, st>>>(a);
-    g_launches.fetch_add(1);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_status(e);
-    // 2) every tile independently
-    if (a.g.ntiles > 0x7fffffffull) return LSCOMP_ERR_ARG;
-    dec_kernel<T, VEC><<<(unsigned)a.g.ntiles, kThreads, 0, st>>>(a);
-    g_launches.fetch_add(1);
-    return cuda_status(cudaGetLastError());
-}
-
-int read_ctl(lscomp_workspace *ws, cudaStream_t st)
-{
-    cudaError_t e = cudaMemcpyAsync(ws->h_ctl, ws->ctl, sizeof(LaunchCtl), cudaMemcpyDeviceToHost, st);
-    if (e != cudaSuccess) return cuda_status(e);
-    e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return cuda_status(e);
-    return dev_status(ws->h_ctl->error);
-}
 
 template <typename T>
 int compress_async_t(lscomp_workspace *ws, const T *d_in, uint32_t x, uint32_t y, uint32_t z, const uint32_t bins[4],
@@ -266,10 +46,10 @@ int compress_async_t(lscomp_workspace *ws, const T *d_in, uint32_t x, uint32_t y
         a.sizes_out = reinterpret_cast<unsigned long long *>(d_sizes);
         const bool pool = a.c.pool_min <= 64;
         switch (vec_class(d_in, z, sizeof(T))) {
-        case 16: s = launch_enc_v<T, 16>(a, layout, pool, ws->sm_count, st); break;
-        case 4: s = launch_enc_v<T, 4>(a, layout, pool, ws->sm_count, st); break;
+        case 16: s = launch_enc_v<T, 16, false>(a, layout, pool, ws->sm_count, st); break;
+        case 4: s = launch_enc_v<T, 4, false>(a, layout, pool, ws->sm_count, st); break;
         default:
-            if (sizeof(T) == 2) s = launch_enc_v<T, 2>(a, layout, pool, ws->sm_count, st);
+            if (sizeof(T) == 2) s = launch_enc_v<T, 2, false>(a, layout, pool, ws->sm_count, st);
             else s = LSCOMP_ERR_ARG;
             break;
         }
@@ -412,6 +192,11 @@ int lscomp_workspace_destroy(lscomp_workspace *ws)
     if (ws->state) cudaFree(ws->state);
     if (ws->ctl) cudaFree(ws->ctl);
     if (ws->h_ctl) cudaFreeHost(ws->h_ctl);
+    if (ws->d_stacks) cudaFree(ws->d_stacks);
+    if (ws->h_stacks) cudaFreeHost(ws->h_stacks);
+    if (ws->d_bsizes) cudaFree(ws->d_bsizes);
+    if (ws->h_bsizes) cudaFreeHost(ws->h_bsizes);
+    if (ws->d_tile_stack) cudaFree(ws->d_tile_stack);
     cudaSetDevice(prev);
     delete ws;
     return LSCOMP_OK;
@@ -580,9 +365,9 @@ extern "C" int lscomp_compress_u16_noalloc(const uint16_t *d_in, uint32_t x, uin
     const bool pool = a.c.pool_min <= 64;
     int s;
     switch (vec_class(d_in, z, 2)) {
-    case 16: s = launch_enc_v<uint16_t, 16>(a, layout, pool, d.sm_count, st); break;
-    case 4: s = launch_enc_v<uint16_t, 4>(a, layout, pool, d.sm_count, st); break;
-    default: s = launch_enc_v<uint16_t, 2>(a, layout, pool, d.sm_count, st); break;
+    case 16: s = launch_enc_v<uint16_t, 16, false>(a, layout, pool, d.sm_count, st); break;
+    case 4: s = launch_enc_v<uint16_t, 4, false>(a, layout, pool, d.sm_count, st); break;
+    default: s = launch_enc_v<uint16_t, 2, false>(a, layout, pool, d.sm_count, st); break;
     }
     if (s) return s;
     LaunchCtl h;  // plain host memory: the copy allocates nothing

@@ -126,7 +126,27 @@ struct EncArgs {
     unsigned long long *state;
     uint32_t epoch;
     unsigned long long *sizes_out;  // optional device copy of {stream_len, payload}
+    // batch launches: the stacks, the stack of every tile (tiles of all
+    // stacks numbered in stack order) and their total; g, in, out, cap and
+    // sizes_out above are unused then
+    const struct BatchStack *stacks;
+    const uint32_t *tile_stack;
+    unsigned long long ntiles_all;
 };
+
+// One stack of a batch launch (device memory).  Its tiles are the tiles
+// tile0 .. tile0 + g.ntiles - 1 of the batch; sizes receives
+// {stream_len, payload} when its last tile is written.
+struct BatchStack {
+    Geom g;
+    const void *in;
+    uint8_t *out;
+    unsigned long long cap;
+    unsigned long long tile0;
+    unsigned long long *sizes;
+};
+
+constexpr unsigned long long kMarker = ~0ull;  // ring entry that ends a CTA's tiles
 
 template <typename T>
 struct DecArgs {
@@ -585,6 +605,13 @@ struct EncSmem {
     // previous one): the phase before entry k's belongs to the group's own
     // entry k - 2 kInStages, which it has already consumed.
     uint64_t in_full2[kInStages];
+    // batch launches: the stack of each input slot and of each payload slot
+    Geom in_geom[kInStages];
+    const BatchStack *in_stack[kInStages];
+    uint8_t *in_out[kInStages];
+    unsigned long long in_gtile[kInStages];   // tile index over the batch (look-back state)
+    const BatchStack *st_stack[kStStages];
+    unsigned long long st_gtile[kStStages];
 };
 
 // The landing barrier of ring entry k and the parity of its phase.
@@ -659,11 +686,10 @@ __device__ __forceinline__ unsigned long long tile_prefix(unsigned long long *st
 // block-row starts of the tile are computed one per lane, so the warp's
 // dependent chain is that of a single block-row.
 template <typename T>
-__device__ void enc_issue(const EncArgs<T> &a, EncSmem &sm, int s, unsigned long long t, uint64_t *full,
+__device__ void enc_issue(const Geom &g, const T *in, EncSmem &sm, int s, unsigned long long t, uint64_t *full,
                           uint32_t lane)
 {
-    const Geom &g = a.g;
-    if (t >= g.ntiles) {
+    if (t == kMarker) {
         if (lane == 0) {
             sm.in_tile[s] = t;
             mbar_arrive(full);
@@ -708,7 +734,7 @@ __device__ void enc_issue(const EncArgs<T> &a, EncSmem &sm, int s, unsigned long
         es = (r0 + lane) * g.Z + col0;
         ne = col1 - col0;
     }
-    const uintptr_t base = reinterpret_cast<uintptr_t>(a.in);
+    const uintptr_t base = reinterpret_cast<uintptr_t>(in);
     const uintptr_t A0 = (base + 15) & ~(uintptr_t)15;
     const uintptr_t A1 = (base + ES * g.N) & ~(uintptr_t)15;
     uint32_t tx = 0;
@@ -946,11 +972,10 @@ __device__ __forceinline__ void block_pack(const Row<T> &A0, const Row<T> &B0, u
 // with another's.  Per tile: pass A from the input ring into registers and
 // header bytes, tile scan and aggregate publication, pass B into the
 // payload ring.
-template <typename T, int VEC, int BINS, bool POOL, int GRP, int WPG>
+template <typename T, int VEC, int BINS, bool POOL, int GRP, int WPG, bool BATCH>
 __device__ __forceinline__ void enc_compute(const EncArgs<T> &a, EncSmem &sm)
 {
     constexpr int UMAX = (Elem<T>::kTileBlocks / 8 + WPG - 1) / WPG;  // units per warp per tile
-    const Geom &g = a.g;
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t grp = warp / WPG, wg = warp % WPG, gtid = tid - grp * WPG * 32;
     const uint32_t barid = kComputeBarrier + grp;
@@ -963,8 +988,8 @@ __device__ __forceinline__ void enc_compute(const EncArgs<T> &a, EncSmem &sm)
         const uint32_t m = k / kStStages;
         bool ok = mbar_wait(entry_full(sm, k), entry_parity(k), a.ctl);
         if (!group_bar_and(barid, WPG * 32, ok)) break;
-        const unsigned long long t = sm.in_tile[i];
-        if (t >= g.ntiles) {
+        const unsigned long long t = sm.in_tile[i];  // tile index inside its stack
+        if (t == kMarker) {
             // end of this CTA's tiles: hand an end marker to the writer
             if (gtid == 0 && mbar_wait(&sm.st_empty[j], (m & 1u) ^ 1u, a.ctl)) {
                 sm.st_tile[j] = t;
@@ -972,6 +997,13 @@ __device__ __forceinline__ void enc_compute(const EncArgs<T> &a, EncSmem &sm)
             }
             break;
         }
+        // the slot's batch fields are read before the slot is released after
+        // pass A (the producer may refill it while this tile is packed);
+        // g is only used in pass A
+        const Geom &g = BATCH ? sm.in_geom[i] : a.g;
+        uint8_t *const out = BATCH ? sm.in_out[i] : a.out;
+        const BatchStack *const bstack = BATCH ? sm.in_stack[i] : nullptr;
+        const unsigned long long gt = BATCH ? sm.in_gtile[i] : t;  // look-back state of the tile
         const TileInfo ti = tile_info(g, t);
         const uint8_t *stage = sm.in[i];
 
@@ -1011,10 +1043,10 @@ __device__ __forceinline__ void enc_compute(const EncArgs<T> &a, EncSmem &sm)
             const uint32_t agg = tile_scan(hdr, off, ti.nblk);
             if (lane == 0) {
                 sm.agg[grp] = agg;
-                st_relaxed_u64(a.state + t, make_state(a.epoch, t == 0 ? kFlagIncl : kFlagAgg, agg));
+                st_relaxed_u64(a.state + gt, make_state(a.epoch, t == 0 ? kFlagIncl : kFlagAgg, agg));
             }
         }
-        for (uint32_t b = gtid; b < ti.nblk; b += WPG * 32) a.out[ti.k0 + b] = hdr[b];
+        for (uint32_t b = gtid; b < ti.nblk; b += WPG * 32) out[ti.k0 + b] = hdr[b];
         bool free_ok = true;
         if (gtid == 0) free_ok = mbar_wait(&sm.st_empty[j], (m & 1u) ^ 1u, a.ctl);
         if (!group_bar_and(barid, WPG * 32, free_ok)) break;
@@ -1035,6 +1067,10 @@ __device__ __forceinline__ void enc_compute(const EncArgs<T> &a, EncSmem &sm)
         if (gtid == 0) {
             sm.st_tile[j] = t;
             sm.st_agg[j] = sm.agg[grp];
+            if (BATCH) {
+                sm.st_stack[j] = bstack;
+                sm.st_gtile[j] = gt;
+            }
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(&sm.st_full[j]);
@@ -1043,10 +1079,34 @@ __device__ __forceinline__ void enc_compute(const EncArgs<T> &a, EncSmem &sm)
 
 // Producer warp: claims tiles in ticket order and fills the input ring;
 // after the last tile, one end marker per compute group.
-template <typename T, int GRP>
+// Batch launches: copy the stack of tile gt (over the batch) into input
+// slot s and return the tile's index inside its stack and its input.
+template <typename T>
+__device__ __forceinline__ unsigned long long batch_slot(const EncArgs<T> &a, EncSmem &sm, int s,
+                                                         unsigned long long gt, const T *&in, uint32_t lane)
+{
+    const BatchStack *st = a.stacks + a.tile_stack[gt];
+    constexpr uint32_t kWords = sizeof(Geom) / 4;
+    static_assert(sizeof(Geom) % 4 == 0, "geometry copied in words");
+    const uint32_t *src = reinterpret_cast<const uint32_t *>(&st->g);
+    uint32_t *dst = reinterpret_cast<uint32_t *>(&sm.in_geom[s]);
+    for (uint32_t w = lane; w < kWords; w += 32) dst[w] = src[w];
+    if (lane == 0) {
+        sm.in_stack[s] = st;
+        sm.in_out[s] = st->out;
+        sm.in_gtile[s] = gt;
+    }
+    in = static_cast<const T *>(st->in);
+    const unsigned long long t = gt - st->tile0;
+    __syncwarp();
+    return t;
+}
+
+template <typename T, int GRP, bool BATCH>
 __device__ __forceinline__ void enc_producer(const EncArgs<T> &a, EncSmem &sm)
 {
     const uint32_t lane = threadIdx.x & 31;
+    const unsigned long long ntiles = BATCH ? a.ntiles_all : a.g.ntiles;
     uint32_t k = 0, ends = 0;
     unsigned long long next = 0;  // the next tile, claimed one tile ahead
     if (lane == 0) next = atomicAdd(&a.ctl->ticket, 1ull);
@@ -1056,14 +1116,21 @@ __device__ __forceinline__ void enc_producer(const EncArgs<T> &a, EncSmem &sm)
         bool ok = mbar_wait(&sm.in_empty[i], (n & 1u) ^ 1u, a.ctl);
         if (!__all_sync(0xffffffffu, ok)) break;
         unsigned long long t = __shfl_sync(0xffffffffu, next, 0);
-        if (t < a.g.ntiles) {
+        const bool real = t < ntiles;
+        if (real) {
             if (lane == 0) next = atomicAdd(&a.ctl->ticket, 1ull);
         } else {
-            t = a.g.ntiles;
+            t = kMarker;
         }
         __syncwarp();
-        enc_issue<T>(a, sm, i, t, entry_full(sm, k), lane);  // the whole warp
-        if (t >= a.g.ntiles && ++ends == (uint32_t)GRP) {
+        if (BATCH && real) {
+            const T *in;
+            t = batch_slot<T>(a, sm, i, t, in, lane);
+            enc_issue<T>(sm.in_geom[i], in, sm, i, t, entry_full(sm, k), lane);  // the whole warp
+        } else {
+            enc_issue<T>(a.g, a.in, sm, i, t, entry_full(sm, k), lane);  // the whole warp
+        }
+        if (!real && ++ends == (uint32_t)GRP) {
             k++;
             break;
         }
@@ -1075,10 +1142,9 @@ __device__ __forceinline__ void enc_producer(const EncArgs<T> &a, EncSmem &sm)
 // for the tile's stream offset (bounded below by this writer's previous
 // tile, whose inclusive prefix it published itself), publication of the
 // inclusive prefix, and the copy of the packed payload to the stream.
-template <typename T>
+template <typename T, bool BATCH>
 __device__ __forceinline__ void enc_writer(const EncArgs<T> &a, EncSmem &sm, uint32_t w)
 {
-    const Geom &g = a.g;
     const uint32_t lane = threadIdx.x & 31;
     long long floor = -1;               // this writer's previous tile
     unsigned long long floor_incl = 0;  // and its inclusive prefix
@@ -1087,30 +1153,35 @@ __device__ __forceinline__ void enc_writer(const EncArgs<T> &a, EncSmem &sm, uin
         const uint32_t m = k / kStStages;
         bool ok = mbar_wait(&sm.st_full[j], m & 1u, a.ctl);
         if (!__all_sync(0xffffffffu, ok)) break;
-        const unsigned long long t = sm.st_tile[j];
-        if (t >= g.ntiles) break;
+        const unsigned long long t = sm.st_tile[j];  // tile index inside its stack
+        if (t == kMarker) break;
+        const BatchStack *bs = BATCH ? sm.st_stack[j] : nullptr;
+        const Geom &g = BATCH ? bs->g : a.g;
+        uint8_t *const out = BATCH ? bs->out : a.out;
+        const unsigned long long cap = BATCH ? bs->cap : a.cap;
+        const unsigned long long gt = BATCH ? sm.st_gtile[j] : t;  // look-back state of the tile
         const uint32_t agg = sm.st_agg[j];
         unsigned long long excl = 0;
         if (t > 0) {
             bool lok = true;
 #if LSC_LOOKBACK
-            excl = lookback_floor(a.state, (long long)t, floor, floor_incl, a.epoch, a.ctl, lok);
+            excl = lookback_floor(a.state, (long long)gt, floor, floor_incl, a.epoch, a.ctl, lok);
 #else
-            excl = lookback_warp(a.state, t, a.epoch, a.ctl, lok);
+            excl = lookback_warp(a.state, gt, a.epoch, a.ctl, lok);
 #endif
             if (!lok) break;
-            if (lane == 0) st_relaxed_u64(a.state + t, make_state(a.epoch, kFlagIncl, excl + agg));
+            if (lane == 0) st_relaxed_u64(a.state + gt, make_state(a.epoch, kFlagIncl, excl + agg));
         }
-        floor = (long long)t;
+        floor = (long long)gt;
         floor_incl = excl + agg;
-        if (g.R + excl + agg > a.cap) {
+        if (g.R + excl + agg > cap) {
             if (lane == 0) raise_error(a.ctl, DEV_ERR_CAPACITY);
             break;
         }
         // copy [0, agg) of the ring slot to out + R + excl (4-byte aligned):
         // 4-byte words up to the first 16-byte boundary, 16-byte stores after
         const uint8_t *src = sm.st[j];
-        uint8_t *dst = a.out + g.R + excl;
+        uint8_t *dst = out + g.R + excl;
         uint32_t head = (uint32_t)((16u - ((uintptr_t)dst & 15u)) & 15u);
         if (head > agg) head = agg;
         if (lane < head / 4u) reinterpret_cast<uint32_t *>(dst)[lane] = reinterpret_cast<const uint32_t *>(src)[lane];
@@ -1125,21 +1196,26 @@ __device__ __forceinline__ void enc_writer(const EncArgs<T> &a, EncSmem &sm, uin
             reinterpret_cast<uint32_t *>(dst + tail)[lane] = reinterpret_cast<const uint32_t *>(src + tail)[lane];
         if (t == g.ntiles - 1) {
             if (lane == 0) {
-                a.ctl->total = excl + agg;
-                a.ctl->stream_len = g.R + excl + agg;
-                if (a.sizes_out) {
-                    a.sizes_out[0] = g.R + excl + agg;
-                    a.sizes_out[1] = excl + agg;
+                if (BATCH) {
+                    bs->sizes[0] = g.R + excl + agg;
+                    bs->sizes[1] = excl + agg;
+                } else {
+                    a.ctl->total = excl + agg;
+                    a.ctl->stream_len = g.R + excl + agg;
+                    if (a.sizes_out) {
+                        a.sizes_out[0] = g.R + excl + agg;
+                        a.sizes_out[1] = excl + agg;
+                    }
                 }
             }
-            if (lane < (uint32_t)(g.R - g.nb)) a.out[g.nb + lane] = 0;  // header pad
+            if (lane < (uint32_t)(g.R - g.nb)) out[g.nb + lane] = 0;  // header pad
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(&sm.st_empty[j]);
     }
 }
 
-template <typename T, int VEC, int BINS, bool POOL, int GRP, int WPG>
+template <typename T, int VEC, int BINS, bool POOL, int GRP, int WPG, bool BATCH>
 __global__ void __launch_bounds__(EncShape<GRP, WPG>::kThreads, 1) enc_kernel(const EncArgs<T> a)
 {
     using S = EncShape<GRP, WPG>;
@@ -1163,11 +1239,11 @@ __global__ void __launch_bounds__(EncShape<GRP, WPG>::kThreads, 1) enc_kernel(co
     }
     __syncthreads();
     if (warp < (uint32_t)S::kCompute)
-        enc_compute<T, VEC, BINS, POOL, GRP, WPG>(a, sm);
+        enc_compute<T, VEC, BINS, POOL, GRP, WPG, BATCH>(a, sm);
     else if (warp == (uint32_t)S::kProducerWarp)
-        enc_producer<T, GRP>(a, sm);
+        enc_producer<T, GRP, BATCH>(a, sm);
     else
-        enc_writer<T>(a, sm, warp - (uint32_t)S::kWriterWarp0);
+        enc_writer<T, BATCH>(a, sm, warp - (uint32_t)S::kWriterWarp0);
     __syncthreads();
     // After an error a load may still be in flight into a slot nobody
     // consumed; the last fill of every slot must land before the CTA's

@@ -51,6 +51,12 @@ _lib = None
 _synth_lib = None
 
 
+class LscompStack(ctypes.Structure):
+    """struct lscomp_stack of include/lscomp.h (one stack of a batch)."""
+    _fields_ = [("d_in", ctypes.c_void_p), ("x", ctypes.c_uint32), ("y", ctypes.c_uint32), ("z", ctypes.c_uint32),
+                ("d_out", ctypes.c_void_p), ("cap", ctypes.c_uint64)]
+
+
 def _u32(x):
     return ctypes.c_uint32(int(x))
 
@@ -87,6 +93,9 @@ def load_library() -> ctypes.CDLL:
     lib.lscomp_compress_u32_async.argtypes = [vp, vp, u32, u32, u32, bins_t, f32, vp, u64, vp, vp]
     lib.lscomp_decompress_u32.argtypes = [vp, vp, u64, u32, u32, u32, bins_t, f32, vp, vp]
     lib.lscomp_decompress_u32_async.argtypes = [vp, vp, u64, u32, u32, u32, bins_t, f32, vp, vp]
+    for sfx in ("u16", "u32"):
+        getattr(lib, f"lscomp_compress_batch_{sfx}").argtypes = [vp, ctypes.POINTER(LscompStack), u32, bins_t, f32,
+                                                                 pu64, pu64, vp]
     _lib = lib
     return lib
 
@@ -173,6 +182,30 @@ def compress_into(ws: Workspace, d_in, dims, bins, pooling: float, d_out, stream
         ctypes.byref(sl), ctypes.byref(rs), ctypes.c_void_p(_stream_handle(stream)))
     _check(st, f"lscomp_compress_{_suffix(d_in)}")
     return int(sl.value), int(rs.value)
+
+
+def compress_batch(ws: Workspace, items, bins, pooling: float, stream=None):
+    """Compress many stacks in one launch: items = [(d_in, dims, d_out), ...],
+    all uint16 (int16 tensors) or all uint32 (int32 tensors), with the same
+    bins and pooling threshold.  Returns [(stream_len, ref_size), ...]; each
+    stack's stream is the one compress_into writes for it alone."""
+    lib = load_library()
+    n = len(items)
+    if n == 0:
+        return []
+    sfx = _suffix(items[0][0])
+    arr = (LscompStack * n)()
+    for i, (d_in, dims, d_out) in enumerate(items):
+        if _suffix(d_in) != sfx:
+            raise ValueError("a batch holds one element type")
+        x, y, z = (int(v) for v in dims)
+        arr[i] = LscompStack(d_in.data_ptr(), x, y, z, d_out.data_ptr(), d_out.numel() * d_out.element_size())
+    sl = (ctypes.c_uint64 * n)()
+    rs = (ctypes.c_uint64 * n)()
+    st = getattr(lib, f"lscomp_compress_batch_{sfx}")(ws.handle, arr, n, _bins(bins), ctypes.c_float(pooling), sl, rs,
+                                                      ctypes.c_void_p(_stream_handle(stream)))
+    _check(st, f"lscomp_compress_batch_{sfx}")
+    return [(int(sl[i]), int(rs[i])) for i in range(n)]
 
 
 def compress_async(ws: Workspace, d_in, dims, bins, pooling: float, d_out, d_sizes=None, stream=None):
