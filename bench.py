@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--batch", type=int, default=0,
+                    help="batched-stacks benchmark over this many stacks (its own JSON line)")
     return ap.parse_args()
 
 
@@ -183,11 +185,126 @@ def barrier(world):
         dist.barrier()
 
 
+def batch_workload(n, seed=11):
+    """Seeded batch of detector stacks: frames U{1..16}, frame height and
+    width U{100..1024} (non-multiples of 8 included), half CSSI-like and half
+    XPCS-like."""
+    import lscomp
+
+    rng = np.random.default_rng(seed)
+    stacks = []
+    for i in range(n):
+        dims = (int(rng.integers(1, 17)), int(rng.integers(100, 1025)), int(rng.integers(100, 1025)))
+        kind = "cssi" if i % 2 == 0 else "xpcs"
+        stacks.append((dims, getattr(lscomp, f"synth_{kind}")(dims, seed=seed + i)))
+    return stacks
+
+
+def bench_batch(args, local):
+    """Batched compress: one lscomp_compress_batch_u16 call over all stacks
+    against one call per stack (asynchronous, and synchronous with the size
+    read back as the reference's host API does).  Inputs resident in HBM."""
+    import torch
+
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+    stacks = batch_workload(args.batch)
+    frames = sum(d[0] for d, _ in stacks)
+    nbytes = sum(h.size * 2 for _, h in stacks)
+    # one input and one output buffer, each stack at a 16-byte boundary
+    offs_in, offs_out, n_in, n_out = [], [], 0, 0
+    for dims, h in stacks:
+        offs_in.append(n_in)
+        n_in += (h.size + 7) // 8 * 8
+        nb = dims[0] * ((dims[1] + 7) // 8) * ((dims[2] + 7) // 8)
+        offs_out.append(n_out)
+        n_out += ((nb + 3) // 4 * 4 + 128 * nb + 15) // 16 * 16
+    d_in_all = torch.zeros(n_in, dtype=torch.int16, device=dev)
+    d_out_all = torch.zeros(n_out, dtype=torch.uint8, device=dev)
+    items = []
+    for (dims, h), oi, oo in zip(stacks, offs_in, offs_out):
+        d = d_in_all[oi:oi + h.size]
+        d.copy_(torch.from_numpy(h.view(np.int16)))
+        nb = dims[0] * ((dims[1] + 7) // 8) * ((dims[2] + 7) // 8)
+        items.append((d, dims, d_out_all[oo:oo + (nb + 3) // 4 * 4 + 128 * nb]))
+    config = {"workload": f"{len(stacks)} stacks, frames U{{1..16}}, frame U{{100..1024}}^2 uint16, half CSSI-like "
+                          f"half XPCS-like", "frames": frames, "input_bytes": nbytes,
+              "modes": "lossless -b 1 1 1 1 -p 1; lossy -b 3 5 10 15 -p 0.5"}
+
+    def timed(fn, reps):
+        for _ in range(max(args.warmup, 3)):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ts = []
+        for _ in range(reps):
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return float(np.median(ts))
+
+    res = {}
+    if args.impl == "reference":
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        from oracle import RefLib
+
+        ref = RefLib()
+        for name, bins, p in MODES:
+            def loop_ref():
+                for d_in, dims, d_out in items:
+                    ref.compress(d_in.data_ptr(), d_out.data_ptr(), dims, bins, p, stream=stream.cuda_stream)
+            ms = timed(loop_ref, args.steps)
+            res[name] = {"per_stack_calls_ms": round(ms, 3), "frames_per_s": round(frames / ms * 1e3, 1)}
+        value = res["lossless"]["frames_per_s"]
+        print(json.dumps({"metric": "batched compress frames per second (reference host API, one call per stack)",
+                          "value": value, "unit": "frames/s", "impl": "reference", "higher_is_better": True,
+                          "per_mode": res, "config": config}))
+        return
+    import lscomp
+
+    ws = lscomp.Workspace(local)
+    for name, bins, p in MODES:
+        got = lscomp.compress_batch(ws, items, bins, p)
+        for (d_in, dims, d_out), (sl, rs) in zip(items[:: max(1, len(items) // 16)], got[:: max(1, len(items) // 16)]):
+            chk = torch.zeros(d_out.numel(), dtype=torch.uint8, device=dev)
+            assert lscomp.compress_into(ws, d_in, dims, bins, p, chk) == (sl, rs)
+            assert torch.equal(chk[:sl], d_out[:sl]), "batch stream differs from the single-stack stream"
+        t_batch = timed(lambda: lscomp.compress_batch(ws, items, bins, p), args.steps)
+
+        def loop_async():
+            for d_in, dims, d_out in items:
+                lscomp.compress_async(ws, d_in, dims, bins, p, d_out)
+
+        def loop_sync():
+            for d_in, dims, d_out in items:
+                lscomp.compress_into(ws, d_in, dims, bins, p, d_out)
+
+        t_async = timed(loop_async, args.steps)
+        t_sync = timed(loop_sync, args.steps)
+        res[name] = {"batch_ms": round(t_batch, 3), "per_stack_async_ms": round(t_async, 3),
+                     "per_stack_sync_ms": round(t_sync, 3), "frames_per_s": round(frames / t_batch * 1e3, 1),
+                     "input_gbs": round(nbytes / t_batch / 1e6, 1),
+                     "speedup_vs_per_stack_async": round(t_async / t_batch, 2),
+                     "speedup_vs_per_stack_sync": round(t_sync / t_batch, 2)}
+    print(json.dumps({"metric": "batched compress frames per second (one lscomp_compress_batch_u16 call)",
+                      "value": res["lossless"]["frames_per_s"], "unit": "frames/s", "higher_is_better": True,
+                      "per_mode": res, "config": config, "timing": "CUDA events around each call, median of "
+                      f"{args.steps}; sizes read back to the host inside the batch call"}))
+
+
 def main():
     args = parse()
     dims = tuple(int(v) for v in args.dims.split(",")) if args.dims else DIMS
     rank, world, local = dist_init(args.gpus)
     import torch
+
+    if args.batch:
+        torch.cuda.set_device(local)
+        if rank == 0:
+            bench_batch(args, local)
+        return
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
