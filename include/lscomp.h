@@ -153,6 +153,40 @@ int lscomp_compress_batch_u32(lscomp_workspace *ws, const lscomp_stack *stacks, 
                               const uint32_t bins[4], float pooling, uint64_t *stream_len,
                               uint64_t *ref_size, void *stream);
 
+/* Container (no counterpart in the reference, whose streams carry neither
+   dimensions, bins, pooling threshold nor element type, and whose size is
+   returned out of band).  A container is a 64-byte header -- magic "LSCZ",
+   version 1, element bytes, x y z, bins, pooling, stream length, reference
+   size, CRC-32 of the header, little-endian -- followed by the stream, byte
+   for byte unchanged.  Decompression from a container needs no other
+   argument. */
+typedef struct lscomp_container_info {
+    uint32_t elem_bytes; /* 2 (uint16) or 4 (uint32) */
+    uint32_t x, y, z;
+    uint32_t bins[4];
+    float pooling;
+    uint64_t stream_len; /* bytes of the stream after the header */
+    uint64_t ref_size;   /* the size the reference's host API reports */
+} lscomp_container_info;
+
+uint32_t lscomp_container_header_bytes(void);
+/* Host functions: fill / parse and check a 64-byte header.  read_header
+   takes the container length (or exactly the header length to parse a
+   header alone) and returns LSCOMP_ERR_CORRUPT for a wrong magic, version,
+   checksum, geometry or a body shorter than the recorded stream. */
+int lscomp_container_write_header(uint8_t *hdr, uint32_t elem_bytes, uint32_t x, uint32_t y, uint32_t z,
+                                  const uint32_t bins[4], float pooling, uint64_t stream_len, uint64_t ref_size);
+int lscomp_container_read_header(const uint8_t *hdr, uint64_t len, lscomp_container_info *info);
+/* Compress d_in (elem_bytes 2 or 4) into a container at d_out (4-byte
+   aligned, cap bytes; the stream starts 64 bytes in).  Synchronises. */
+int lscomp_compress_container(lscomp_workspace *ws, uint32_t elem_bytes, const void *d_in, uint32_t x, uint32_t y,
+                              uint32_t z, const uint32_t bins[4], float pooling, uint8_t *d_out, uint64_t cap,
+                              uint64_t *container_len, void *stream);
+/* Decompress a container of len bytes at d_in into d_out (out_cap bytes);
+   *info (may be NULL) receives the header.  Synchronises. */
+int lscomp_decompress_container(lscomp_workspace *ws, const uint8_t *d_in, uint64_t len, void *d_out,
+                                uint64_t out_cap, lscomp_container_info *info, void *stream);
+
 /* Wait for the workspace's last launch on `stream` and return its status. */
 int lscomp_workspace_check(lscomp_workspace *ws, void *stream);
 

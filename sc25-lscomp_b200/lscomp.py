@@ -51,6 +51,17 @@ _lib = None
 _synth_lib = None
 
 
+class ContainerInfo(ctypes.Structure):
+    """struct lscomp_container_info of include/lscomp.h."""
+    _fields_ = [("elem_bytes", ctypes.c_uint32), ("x", ctypes.c_uint32), ("y", ctypes.c_uint32),
+                ("z", ctypes.c_uint32), ("bins", ctypes.c_uint32 * 4), ("pooling", ctypes.c_float),
+                ("stream_len", ctypes.c_uint64), ("ref_size", ctypes.c_uint64)]
+
+    def as_dict(self):
+        return {"elem_bytes": self.elem_bytes, "dims": (self.x, self.y, self.z), "bins": tuple(self.bins),
+                "pooling": self.pooling, "stream_len": self.stream_len, "ref_size": self.ref_size}
+
+
 class LscompStack(ctypes.Structure):
     """struct lscomp_stack of include/lscomp.h (one stack of a batch)."""
     _fields_ = [("d_in", ctypes.c_void_p), ("x", ctypes.c_uint32), ("y", ctypes.c_uint32), ("z", ctypes.c_uint32),
@@ -93,6 +104,11 @@ def load_library() -> ctypes.CDLL:
     lib.lscomp_compress_u32_async.argtypes = [vp, vp, u32, u32, u32, bins_t, f32, vp, u64, vp, vp]
     lib.lscomp_decompress_u32.argtypes = [vp, vp, u64, u32, u32, u32, bins_t, f32, vp, vp]
     lib.lscomp_decompress_u32_async.argtypes = [vp, vp, u64, u32, u32, u32, bins_t, f32, vp, vp]
+    lib.lscomp_container_header_bytes.restype = u32
+    lib.lscomp_container_write_header.argtypes = [vp, u32, u32, u32, u32, bins_t, f32, u64, u64]
+    lib.lscomp_container_read_header.argtypes = [vp, u64, ctypes.POINTER(ContainerInfo)]
+    lib.lscomp_compress_container.argtypes = [vp, u32, vp, u32, u32, u32, bins_t, f32, vp, u64, pu64, vp]
+    lib.lscomp_decompress_container.argtypes = [vp, vp, u64, vp, u64, ctypes.POINTER(ContainerInfo), vp]
     for sfx in ("u16", "u32"):
         getattr(lib, f"lscomp_compress_batch_{sfx}").argtypes = [vp, ctypes.POINTER(LscompStack), u32, bins_t, f32,
                                                                  pu64, pu64, vp]
@@ -206,6 +222,51 @@ def compress_batch(ws: Workspace, items, bins, pooling: float, stream=None):
                                                       ctypes.c_void_p(_stream_handle(stream)))
     _check(st, f"lscomp_compress_batch_{sfx}")
     return [(int(sl[i]), int(rs[i])) for i in range(n)]
+
+
+def container_header(elem_bytes: int, dims, bins, pooling: float, stream_len: int, ref_size: int) -> bytes:
+    """The 64-byte container header for a stream (host only)."""
+    lib = load_library()
+    buf = ctypes.create_string_buffer(int(lib.lscomp_container_header_bytes()))
+    x, y, z = (int(v) for v in dims)
+    _check(lib.lscomp_container_write_header(buf, elem_bytes, x, y, z, _bins(bins), ctypes.c_float(pooling),
+                                             ctypes.c_uint64(stream_len), ctypes.c_uint64(ref_size)),
+           "lscomp_container_write_header")
+    return buf.raw
+
+
+def parse_container(buf: bytes, length: Optional[int] = None) -> dict:
+    """Parse and check a container header (host only); length defaults to
+    len(buf), i.e. a whole container, or a header alone when len(buf) == 64."""
+    lib = load_library()
+    info = ContainerInfo()
+    raw = ctypes.create_string_buffer(bytes(buf), len(buf))
+    _check(lib.lscomp_container_read_header(raw, ctypes.c_uint64(len(buf) if length is None else length),
+                                            ctypes.byref(info)), "lscomp_container_read_header")
+    return info.as_dict()
+
+
+def compress_container(ws: Workspace, d_in, dims, bins, pooling: float, d_out, stream=None) -> int:
+    """Compress into a container (header + unchanged stream) in d_out; returns its length."""
+    lib = load_library()
+    x, y, z = (int(v) for v in dims)
+    n = ctypes.c_uint64(0)
+    _check(lib.lscomp_compress_container(ws.handle, d_in.element_size(), ctypes.c_void_p(d_in.data_ptr()), x, y, z,
+                                         _bins(bins), ctypes.c_float(pooling), ctypes.c_void_p(d_out.data_ptr()),
+                                         ctypes.c_uint64(d_out.numel() * d_out.element_size()), ctypes.byref(n),
+                                         ctypes.c_void_p(_stream_handle(stream))), "lscomp_compress_container")
+    return int(n.value)
+
+
+def decompress_container(ws: Workspace, d_cont, length: int, d_out, stream=None) -> dict:
+    """Decompress a container of `length` bytes into d_out; returns its header."""
+    lib = load_library()
+    info = ContainerInfo()
+    _check(lib.lscomp_decompress_container(ws.handle, ctypes.c_void_p(d_cont.data_ptr()), ctypes.c_uint64(length),
+                                           ctypes.c_void_p(d_out.data_ptr()),
+                                           ctypes.c_uint64(d_out.numel() * d_out.element_size()), ctypes.byref(info),
+                                           ctypes.c_void_p(_stream_handle(stream))), "lscomp_decompress_container")
+    return info.as_dict()
 
 
 def compress_async(ws: Workspace, d_in, dims, bins, pooling: float, d_out, d_sizes=None, stream=None):
