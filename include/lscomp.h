@@ -187,6 +187,37 @@ int lscomp_compress_container(lscomp_workspace *ws, uint32_t elem_bytes, const v
 int lscomp_decompress_container(lscomp_workspace *ws, const uint8_t *d_in, uint64_t len, void *d_out,
                                 uint64_t out_cap, lscomp_container_info *info, void *stream);
 
+/* Serving loop (no counterpart in the reference).  A server owns a device
+   arena of arena_bytes, pinned staging of the same size, a workspace, a
+   CUDA stream and a worker thread.  Any thread submits requests with host
+   buffers; the worker admits waiting requests in arrival order while their
+   worst-case device footprints (input + largest possible output) fit the
+   arena, sends the compress requests of a round that share element type,
+   bins and pooling threshold to the GPU as one batch launch, and decodes
+   the decompress requests.  A compress request produces a container (see
+   above) in h_out; a decompress request takes a container.  Outputs do not
+   depend on what else is in the batch.  Submit returns a request id > 0, or
+   minus a status (LSCOMP_ERR_TOO_LARGE: the footprint exceeds the arena).
+   Caller buffers must stay valid until lscomp_server_wait returns for the
+   request; wait releases the request.  destroy runs what was submitted. */
+typedef struct lscomp_server lscomp_server;
+typedef struct lscomp_server_result {
+    int status;          /* LSCOMP_OK or the request's error */
+    uint64_t out_len;    /* bytes written to h_out */
+    uint64_t queued_ns;  /* submit -> admitted */
+    uint64_t service_ns; /* admitted -> done (copies, kernels, copies) */
+} lscomp_server_result;
+
+int lscomp_server_create(lscomp_server **server, int device, uint64_t arena_bytes);
+int lscomp_server_destroy(lscomp_server *server);
+int64_t lscomp_server_submit_compress(lscomp_server *server, uint32_t elem_bytes, const void *h_in, uint32_t x,
+                                      uint32_t y, uint32_t z, const uint32_t bins[4], float pooling, void *h_out,
+                                      uint64_t out_cap);
+int64_t lscomp_server_submit_decompress(lscomp_server *server, const void *h_container, uint64_t len, void *h_out,
+                                        uint64_t out_cap);
+int lscomp_server_wait(lscomp_server *server, int64_t id, lscomp_server_result *result);
+int lscomp_server_stats(lscomp_server *server, uint64_t *rounds, uint64_t *batches, uint64_t *batched_requests);
+
 /* Wait for the workspace's last launch on `stream` and return its status. */
 int lscomp_workspace_check(lscomp_workspace *ws, void *stream);
 

@@ -62,6 +62,12 @@ class ContainerInfo(ctypes.Structure):
                 "pooling": self.pooling, "stream_len": self.stream_len, "ref_size": self.ref_size}
 
 
+class ServerResult(ctypes.Structure):
+    """struct lscomp_server_result of include/lscomp.h."""
+    _fields_ = [("status", ctypes.c_int), ("out_len", ctypes.c_uint64), ("queued_ns", ctypes.c_uint64),
+                ("service_ns", ctypes.c_uint64)]
+
+
 class LscompStack(ctypes.Structure):
     """struct lscomp_stack of include/lscomp.h (one stack of a batch)."""
     _fields_ = [("d_in", ctypes.c_void_p), ("x", ctypes.c_uint32), ("y", ctypes.c_uint32), ("z", ctypes.c_uint32),
@@ -109,6 +115,14 @@ def load_library() -> ctypes.CDLL:
     lib.lscomp_container_read_header.argtypes = [vp, u64, ctypes.POINTER(ContainerInfo)]
     lib.lscomp_compress_container.argtypes = [vp, u32, vp, u32, u32, u32, bins_t, f32, vp, u64, pu64, vp]
     lib.lscomp_decompress_container.argtypes = [vp, vp, u64, vp, u64, ctypes.POINTER(ContainerInfo), vp]
+    lib.lscomp_server_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, u64]
+    lib.lscomp_server_destroy.argtypes = [vp]
+    lib.lscomp_server_submit_compress.restype = ctypes.c_int64
+    lib.lscomp_server_submit_compress.argtypes = [vp, u32, vp, u32, u32, u32, bins_t, f32, vp, u64]
+    lib.lscomp_server_submit_decompress.restype = ctypes.c_int64
+    lib.lscomp_server_submit_decompress.argtypes = [vp, vp, u64, vp, u64]
+    lib.lscomp_server_wait.argtypes = [vp, ctypes.c_int64, ctypes.POINTER(ServerResult)]
+    lib.lscomp_server_stats.argtypes = [vp, pu64, pu64, pu64]
     for sfx in ("u16", "u32"):
         getattr(lib, f"lscomp_compress_batch_{sfx}").argtypes = [vp, ctypes.POINTER(LscompStack), u32, bins_t, f32,
                                                                  pu64, pu64, vp]
@@ -267,6 +281,65 @@ def decompress_container(ws: Workspace, d_cont, length: int, d_out, stream=None)
                                            ctypes.c_uint64(d_out.numel() * d_out.element_size()), ctypes.byref(info),
                                            ctypes.c_void_p(_stream_handle(stream))), "lscomp_decompress_container")
     return info.as_dict()
+
+
+class Server:
+    """The serving loop of liblscomp.so (lscomp_server_*): submit requests with
+    numpy host buffers from any thread, wait for them in any order.  The
+    buffers are kept alive here until the request is waited for."""
+
+    def __init__(self, device: int = 0, arena_bytes: int = 1 << 30):
+        lib = load_library()
+        h = ctypes.c_void_p()
+        _check(lib.lscomp_server_create(ctypes.byref(h), device, ctypes.c_uint64(arena_bytes)), "lscomp_server_create")
+        self._h = h
+        self._keep = {}
+
+    def submit_compress(self, h_in: np.ndarray, dims, bins, pooling: float, h_out: np.ndarray) -> int:
+        assert h_in.flags["C_CONTIGUOUS"] and h_out.flags["C_CONTIGUOUS"] and h_in.itemsize in (2, 4)
+        x, y, z = (int(v) for v in dims)
+        rid = load_library().lscomp_server_submit_compress(self._h, h_in.itemsize, h_in.ctypes.data, x, y, z,
+                                                           _bins(bins), ctypes.c_float(pooling), h_out.ctypes.data,
+                                                           ctypes.c_uint64(h_out.nbytes))
+        if rid < 0:
+            raise LscompError(int(-rid), "lscomp_server_submit_compress")
+        self._keep[rid] = (h_in, h_out)
+        return int(rid)
+
+    def submit_decompress(self, container: np.ndarray, h_out: np.ndarray) -> int:
+        assert container.flags["C_CONTIGUOUS"] and h_out.flags["C_CONTIGUOUS"]
+        rid = load_library().lscomp_server_submit_decompress(self._h, container.ctypes.data,
+                                                             ctypes.c_uint64(container.nbytes), h_out.ctypes.data,
+                                                             ctypes.c_uint64(h_out.nbytes))
+        if rid < 0:
+            raise LscompError(int(-rid), "lscomp_server_submit_decompress")
+        self._keep[rid] = (container, h_out)
+        return int(rid)
+
+    def wait(self, rid: int) -> dict:
+        r = ServerResult()
+        _check(load_library().lscomp_server_wait(self._h, ctypes.c_int64(rid), ctypes.byref(r)), "lscomp_server_wait")
+        self._keep.pop(rid, None)
+        return {"status": r.status, "out_len": int(r.out_len), "queued_ns": int(r.queued_ns),
+                "service_ns": int(r.service_ns)}
+
+    def stats(self) -> dict:
+        a, b, c = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        _check(load_library().lscomp_server_stats(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)),
+               "lscomp_server_stats")
+        return {"rounds": a.value, "batches": b.value, "batched_requests": c.value}
+
+    def close(self):
+        if self._h:
+            load_library().lscomp_server_destroy(self._h)
+            self._h = None
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def compress_async(ws: Workspace, d_in, dims, bins, pooling: float, d_out, d_sizes=None, stream=None):

@@ -1,0 +1,138 @@
+"""The serving loop (lscomp_server_*): host buffers in and out, admission
+into a fixed device arena, continuous batching of compress requests.
+
+A served request's output must not depend on what it was batched with: every
+served container is compared byte for byte with lscomp_compress_container on
+the same stack alone, and decompress requests with the stack."""
+import threading
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+LOSSLESS = ((1, 1, 1, 1), 1.0)
+LOSSY = ((3, 5, 10, 15), 0.5)
+
+
+@pytest.fixture(scope="module")
+def lz():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import lscomp
+
+    lscomp.load_library()
+    return lscomp
+
+
+def stack(dims, seed, wide=False):
+    rng = np.random.default_rng(seed)
+    a = rng.integers(0, 300, size=dims, dtype=np.uint32 if wide else np.uint16)
+    a[rng.random(dims) < 0.5] = 0
+    return a
+
+
+def alone(lz, ws, a, dims, bins, p):
+    """Container of one stack made by the single-stack call."""
+    view = np.int32 if a.itemsize == 4 else np.int16
+    d_in = torch.from_numpy(np.ascontiguousarray(a).view(view).ravel()).cuda()
+    out = torch.zeros(64 + lz.max_stream_bytes(dims, a.itemsize), dtype=torch.uint8, device="cuda")
+    n = lz.compress_container(ws, d_in, dims, bins, p, out)
+    return out[:n].cpu().numpy()
+
+
+def requests(n, seed):
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        dims = (int(rng.integers(1, 6)), int(rng.integers(1, 300)), int(rng.integers(1, 400)))
+        wide = bool(i % 5 == 4)
+        bins, p = (LOSSLESS, LOSSY, ((5, 10, 15, 20), 0.3))[i % 3]
+        out.append((stack(dims, seed * 1000 + i, wide), dims, bins, p))
+    return out
+
+
+def test_alone_vs_mix_bit_exact(lz):
+    reqs = requests(60, seed=1)
+    ws = lz.Workspace(0)
+    srv = lz.Server(0, arena_bytes=1 << 30)
+    outs, ids = [], []
+    for a, dims, bins, p in reqs:  # all submitted before any is waited for: mixed rounds
+        o = np.zeros(64 + lz.max_stream_bytes(dims, a.itemsize), dtype=np.uint8)
+        outs.append(o)
+        ids.append(srv.submit_compress(a, dims, bins, p, o))
+    res = [srv.wait(i) for i in ids]
+    st = srv.stats()
+    assert st["batched_requests"] == len(reqs) and st["batches"] < len(reqs)  # requests were batched
+    for (a, dims, bins, p), o, r in zip(reqs, outs, res):
+        assert r["status"] == 0
+        ref = alone(lz, ws, a, dims, bins, p)
+        assert r["out_len"] == len(ref)
+        assert np.array_equal(o[: r["out_len"]], ref)
+    # and back: decompress requests of the served containers
+    decs, ids = [], []
+    for (a, dims, bins, p), o, r in zip(reqs, outs, res):
+        d = np.zeros_like(a)
+        decs.append(d)
+        ids.append(srv.submit_decompress(o[: r["out_len"]], d))
+    for (a, dims, bins, p), d, i, o, r in zip(reqs, decs, ids, outs, res):
+        rr = srv.wait(i)
+        assert rr["status"] == 0 and rr["out_len"] == a.nbytes
+        if bins == (1, 1, 1, 1):
+            assert np.array_equal(d, a)
+        else:
+            view = np.int32 if a.itemsize == 4 else np.int16
+            cont = torch.from_numpy(o[: r["out_len"]].copy()).cuda()
+            ref = torch.empty(a.size, dtype=torch.int32 if a.itemsize == 4 else torch.int16, device="cuda")
+            lz.decompress_container(ws, cont, r["out_len"], ref)
+            assert np.array_equal(d.view(view).ravel(), ref.cpu().numpy())
+    srv.close()
+
+
+def test_admission_small_arena(lz):
+    # the arena holds only a few requests at a time: many rounds, same outputs
+    reqs = requests(40, seed=2)
+    ws = lz.Workspace(0)
+    srv = lz.Server(0, arena_bytes=8 << 20)
+    outs = [np.zeros(64 + lz.max_stream_bytes(d, a.itemsize), dtype=np.uint8) for a, d, _, _ in reqs]
+    ids = [srv.submit_compress(a, d, b, p, o) for (a, d, b, p), o in zip(reqs, outs)]
+    res = [srv.wait(i) for i in ids]
+    assert srv.stats()["rounds"] > 1
+    for (a, d, b, p), o, r in zip(reqs, outs, res):
+        assert r["status"] == 0
+        assert np.array_equal(o[: r["out_len"]], alone(lz, ws, a, d, b, p))
+    # larger than the whole arena: refused at submission
+    big = np.zeros((16, 512, 512), dtype=np.uint16)
+    with pytest.raises(lz.LscompError) as e:
+        srv.submit_compress(big, big.shape, *LOSSLESS, np.zeros(1 << 24, dtype=np.uint8))
+    assert e.value.status == 8
+    # output buffer too small for the container: that request fails alone
+    a, d, b, p = reqs[0]
+    rid = srv.submit_compress(a, d, b, p, np.zeros(70, dtype=np.uint8))
+    assert srv.wait(rid)["status"] == 2
+    srv.close()
+
+
+def test_threads(lz):
+    reqs = requests(48, seed=3)
+    ws = lz.Workspace(0)
+    srv = lz.Server(0, arena_bytes=256 << 20)
+    outs = [np.zeros(64 + lz.max_stream_bytes(d, a.itemsize), dtype=np.uint8) for a, d, _, _ in reqs]
+    results = [None] * len(reqs)
+
+    def client(k):
+        for i in range(k, len(reqs), 4):
+            a, d, b, p = reqs[i]
+            results[i] = srv.wait(srv.submit_compress(a, d, b, p, outs[i]))
+
+    th = [threading.Thread(target=client, args=(k,)) for k in range(4)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    for (a, d, b, p), o, r in zip(reqs, outs, results):
+        assert r["status"] == 0
+        assert np.array_equal(o[: r["out_len"]], alone(lz, ws, a, d, b, p))
+    srv.close()
