@@ -49,6 +49,9 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--serve", type=float, default=0.0,
+                    help="serving benchmark: Poisson arrivals at this many requests per second (its own JSON line)")
+    ap.add_argument("--serve-seconds", type=float, default=10.0)
     ap.add_argument("--batch", type=int, default=0,
                     help="batched-stacks benchmark over this many stacks (its own JSON line)")
     return ap.parse_args()
@@ -294,6 +297,95 @@ def bench_batch(args, local):
                       f"{args.steps}; sizes read back to the host inside the batch call"}))
 
 
+def bench_serve(args, local):
+    """Serving loop under Poisson arrivals: requests of log-uniform size
+    (256 KB .. 64 MB of 1024x1024 or 1813x1558 uint16 frames), 70% compress /
+    30% decompress, 60% lossless / 40% lossy (-b 3 5 10 15 -p 0.5), host
+    buffers in and out.  Latency = queue + service time per request."""
+    import lscomp
+
+    rng = np.random.default_rng(5)
+    pool = []
+    for i in range(24):
+        size = float(np.exp(rng.uniform(np.log(256 << 10), np.log(64 << 20))))
+        h, w = (1024, 1024) if i % 2 else (1813, 1558)
+        frames = max(1, int(round(size / (2 * h * w))))
+        if size < 2 * h * w:
+            h = max(8, int(size / (2 * w)))
+        dims = (frames, h, w)
+        kind = "xpcs" if i % 2 else "cssi"
+        pool.append((dims, getattr(lscomp, f"synth_{kind}")(dims, seed=100 + i).reshape(dims)))
+    modes = [("lossless", (1, 1, 1, 1), 1.0), ("lossy", (3, 5, 10, 15), 0.5)]
+    arena = 8 << 30
+    srv = lscomp.Server(local, arena_bytes=arena)
+    # containers of every pool stack in both modes, for the decompress requests
+    conts = {}
+    for k, (dims, a) in enumerate(pool):
+        for name, bins, p in modes:
+            o = np.zeros(64 + lscomp.max_stream_bytes(dims), dtype=np.uint8)
+            r = srv.wait(srv.submit_compress(a, dims, bins, p, o))
+            conts[(k, name)] = o[: r["out_len"]].copy()
+    import threading
+    import queue as qmod
+
+    pending = qmod.Queue()
+    lat, nbytes_done = [], [0]
+
+    def waiter():
+        while True:
+            item = pending.get()
+            if item is None:
+                return
+            rid, nb = item
+            r = srv.wait(rid)
+            if r["status"] != 0:
+                raise SystemExit(f"request failed: {r}")
+            lat.append((r["queued_ns"] + r["service_ns"]) / 1e6)
+            nbytes_done[0] += nb
+
+    wt = threading.Thread(target=waiter)
+    wt.start()
+    rate, dur = args.serve, args.serve_seconds
+    t0 = time.perf_counter()
+    t_next = t0
+    n_sub = 0
+    while True:
+        t_next += float(rng.exponential(1.0 / rate))
+        if t_next - t0 > dur:
+            break
+        while time.perf_counter() < t_next:
+            pass
+        k = int(rng.integers(0, len(pool)))
+        dims, a = pool[k]
+        name, bins, p = modes[0] if rng.random() < 0.6 else modes[1]
+        if rng.random() < 0.7:
+            o = np.empty(64 + lscomp.max_stream_bytes(dims), dtype=np.uint8)
+            rid = srv.submit_compress(a, dims, bins, p, o)
+        else:
+            o = np.empty_like(a)
+            rid = srv.submit_decompress(conts[(k, name)], o)
+        pending.put((rid, a.nbytes))
+        n_sub += 1
+    pending.put(None)
+    wt.join()
+    elapsed = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    lat_a = np.array(lat)
+    print(json.dumps({"metric": "serving latency p99 (Poisson arrivals, host buffers in and out)",
+                      "value": round(float(np.percentile(lat_a, 99)), 3), "unit": "ms", "higher_is_better": False,
+                      "p50_ms": round(float(np.percentile(lat_a, 50)), 3),
+                      "p99_ms": round(float(np.percentile(lat_a, 99)), 3),
+                      "mean_ms": round(float(lat_a.mean()), 3), "requests": n_sub,
+                      "offered_req_per_s": rate, "achieved_req_per_s": round(n_sub / elapsed, 1),
+                      "input_gb_per_s": round(nbytes_done[0] / elapsed / 1e9, 2),
+                      "rounds": st["rounds"], "batches": st["batches"], "batched_requests": st["batched_requests"],
+                      "config": {"workload": "24 seeded stacks, log-uniform 256 KB..64 MB, 1024x1024 (XPCS-like) or "
+                                             "1813x1558 (CSSI-like) uint16 frames; 70/30 compress/decompress; "
+                                             "60/40 lossless/lossy", "arena_bytes": arena,
+                                 "duration_s": dur}}))
+
+
 def main():
     args = parse()
     dims = tuple(int(v) for v in args.dims.split(",")) if args.dims else DIMS
@@ -304,6 +396,11 @@ def main():
         torch.cuda.set_device(local)
         if rank == 0:
             bench_batch(args, local)
+        return
+    if args.serve:
+        torch.cuda.set_device(local)
+        if rank == 0:
+            bench_serve(args, local)
         return
 
     torch.cuda.set_device(local)

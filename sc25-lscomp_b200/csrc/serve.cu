@@ -17,8 +17,9 @@
 //     launch (lscomp_compress_batch_*), whatever their shapes; decompress
 //     requests of the round run one after the other;
 //   * staging: inputs and outputs pass through pinned host memory of the
-//     arena's size, so the copies run at PCIe/NVLink-C2C speed from pageable
-//     caller buffers;
+//     arena's size, so the device copies run at full link speed from
+//     pageable caller buffers; the host-side copies of a round are split
+//     over a pool of copy threads;
 //   * every request records its time in the queue and in service.
 //
 // A request's output depends only on the request: batched or alone, its
@@ -31,6 +32,7 @@
 #include <deque>
 #include <mutex>
 #include <thread>
+#include <tuple>
 #include <unordered_map>
 #include <vector>
 #include "lscomp.h"
@@ -68,6 +70,69 @@ struct Request {
     uint64_t footprint() const { return align_up(in_bytes) + align_up(out_dev); }
 };
 
+// A fixed pool of host threads that runs lists of memcpy jobs, split into
+// chunks of at most kChunk bytes.
+class CopyPool {
+  public:
+    explicit CopyPool(unsigned n)
+    {
+        for (unsigned i = 0; i < n; i++) th_.emplace_back([this] { run(); });
+    }
+    ~CopyPool()
+    {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto &t : th_) t.join();
+    }
+    // copy every (dst, src, n) of the list; returns when all are done
+    void copy(const std::vector<std::tuple<void *, const void *, uint64_t>> &jobs)
+    {
+        std::unique_lock<std::mutex> lk(mu_);
+        for (const auto &j : jobs) {
+            uint8_t *d = static_cast<uint8_t *>(std::get<0>(j));
+            const uint8_t *s = static_cast<const uint8_t *>(std::get<1>(j));
+            for (uint64_t o = 0, n = std::get<2>(j); o < n; o += kChunk)
+                work_.push_back({d + o, s + o, n - o < kChunk ? n - o : kChunk});
+        }
+        pending_ += work_.size();
+        cv_.notify_all();
+        done_cv_.wait(lk, [&] { return pending_ == 0; });
+    }
+
+  private:
+    static constexpr uint64_t kChunk = 4ull << 20;
+    struct Job {
+        uint8_t *d;
+        const uint8_t *s;
+        uint64_t n;
+    };
+    void run()
+    {
+        std::unique_lock<std::mutex> lk(mu_);
+        for (;;) {
+            cv_.wait(lk, [&] { return stop_ || !work_.empty(); });
+            if (work_.empty()) return;
+            Job j = work_.front();
+            work_.pop_front();
+            lk.unlock();
+            memcpy(j.d, j.s, j.n);
+            lk.lock();
+            if (--pending_ == 0) done_cv_.notify_all();
+        }
+    }
+    std::vector<std::thread> th_;
+    std::deque<Job> work_;
+    uint64_t pending_ = 0;
+    bool stop_ = false;
+    std::mutex mu_;
+    std::condition_variable cv_, done_cv_;
+};
+
+constexpr unsigned kCopyThreads = 8;
+
 }  // namespace
 
 struct lscomp_server {
@@ -85,6 +150,7 @@ struct lscomp_server {
     bool stop = false;
     int64_t next_id = 1;
     uint64_t rounds = 0, batches = 0, batched_requests = 0;
+    CopyPool *copies = nullptr;
 };
 
 namespace {
@@ -109,12 +175,15 @@ void run_round(lscomp_server *s, std::vector<Request *> &round)
         out_off[i] = off;
         off += align_up(round[i]->out_dev);
     }
-    // inputs: caller -> pinned staging -> device
+    // inputs: caller -> pinned staging (copy threads) -> device
     std::vector<int> st(round.size(), LSCOMP_OK);
+    {
+        std::vector<std::tuple<void *, const void *, uint64_t>> jobs;
+        for (size_t i = 0; i < round.size(); i++) jobs.emplace_back(s->staging + in_off[i], round[i]->h_in, round[i]->in_bytes);
+        s->copies->copy(jobs);
+    }
     for (size_t i = 0; i < round.size(); i++) {
-        Request *r = round[i];
-        memcpy(s->staging + in_off[i], r->h_in, r->in_bytes);
-        if (cudaMemcpyAsync(s->arena + in_off[i], s->staging + in_off[i], r->in_bytes, cudaMemcpyHostToDevice,
+        if (cudaMemcpyAsync(s->arena + in_off[i], s->staging + in_off[i], round[i]->in_bytes, cudaMemcpyHostToDevice,
                             s->st) != cudaSuccess)
             st[i] = LSCOMP_ERR_CUDA;
     }
@@ -182,12 +251,17 @@ void run_round(lscomp_server *s, std::vector<Request *> &round)
             st[i] = LSCOMP_ERR_CUDA;
     }
     const int sync = cudaStreamSynchronize(s->st) == cudaSuccess ? LSCOMP_OK : LSCOMP_ERR_CUDA;
-    // outputs: pinned staging -> caller
+    // outputs: pinned staging -> caller (copy threads)
+    {
+        std::vector<std::tuple<void *, const void *, uint64_t>> jobs;
+        for (size_t i = 0; i < round.size(); i++)
+            if (!(st[i] ? st[i] : sync)) jobs.emplace_back(round[i]->h_out, s->staging + out_off[i], round[i]->out_len);
+        s->copies->copy(jobs);
+    }
     std::lock_guard<std::mutex> lk(s->mu);
     for (size_t i = 0; i < round.size(); i++) {
         Request *r = round[i];
         int status = st[i] ? st[i] : sync;
-        if (!status) memcpy(r->h_out, s->staging + out_off[i], r->out_len);
         finish(s, r, status, status ? 0 : r->out_len);
     }
     s->rounds++;
@@ -263,6 +337,7 @@ int lscomp_server_create(lscomp_server **out, int device, uint64_t arena_bytes)
         lscomp_server_destroy(s);
         return st;
     }
+    s->copies = new CopyPool(kCopyThreads);
     s->worker = std::thread(worker_main, s);
     *out = s;
     return LSCOMP_OK;
@@ -277,6 +352,7 @@ int lscomp_server_destroy(lscomp_server *s)
         s->cv_work.notify_all();
     }
     if (s->worker.joinable()) s->worker.join();  // runs what was submitted
+    delete s->copies;
     int prev = 0;
     cudaGetDevice(&prev);
     cudaSetDevice(s->device);
