@@ -623,12 +623,19 @@ __device__ __forceinline__ uint64_t *entry_full(EncSmem &sm, uint32_t k)
 
 __device__ __forceinline__ uint32_t entry_parity(uint32_t k) { return (k / (2 * kInStages)) & 1u; }
 
+// payload bytes of one tile at most (uint16: 256 blocks x 16 planes x 8
+// bytes; uint32: 128 blocks x 31 planes x 8 bytes)
+constexpr uint32_t kMaxTilePayload = 32768;
+
 struct DecSmem {
+    alignas(16) uint8_t pay[kMaxTilePayload + 32];  // the tile's payload (TMA destination)
+    uint64_t pay_full;                               // its landing
     uint32_t br_rel[kMaxTileBlocks];
     uint8_t br_rows[kMaxTileBlocks];
     uint8_t hdr[kMaxTileBlocks];
     uint32_t off[kMaxTileBlocks];
     unsigned long long base;
+    uint32_t pay_mis;                                // byte offset of the payload's first byte in pay
     uint32_t flag_ok;
 };
 
@@ -1305,6 +1312,7 @@ __global__ void __launch_bounds__(kThreads) dec_offsets_kernel(const DecArgs<T> 
             bool lok;
             const unsigned long long base = tile_prefix(a.state, sg, a.epoch, agg, a.ctl, lok);
             if (lok && t0 + lane < g.ntiles) a.tile_off[t0 + lane] = base + (inc - v);
+            if (lok && t0 + lane == g.ntiles - 1) a.tile_off[g.ntiles] = base + inc;  // end of the payload
             if (lane == 0) ok_s = lok ? 1u : 0u;
         }
         __syncthreads();
@@ -1419,6 +1427,36 @@ __global__ void __launch_bounds__(kThreads, LSC_DEC_HOIST ? 3 : 4) dec_kernel(co
     const unsigned long long t = blockIdx.x;
     if (t >= g.ntiles) return;
 
+    // thread 0: the tile's payload [R + tile_off[t], R + tile_off[t+1]) into
+    // shared memory with one bulk copy, overlapping the header scan; the
+    // range is clamped to the readable stream and to one tile's maximum
+    if (tid == 0) {
+        mbar_init(&sm.pay_full, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        const unsigned long long b0 = a.tile_off[t], b1 = a.tile_off[t + 1];
+        uint32_t tx = 0;
+        sm.pay_mis = 0;
+        if (b1 >= b0 && b1 - b0 <= kMaxTilePayload && g.R + b1 <= a.cap) {
+            const uintptr_t base = reinterpret_cast<uintptr_t>(a.in);
+            const uintptr_t A0 = (base + 15) & ~(uintptr_t)15;
+            const uintptr_t A1 = (base + a.cap) & ~(uintptr_t)15;
+            const uintptr_t ga = base + g.R + b0, ge = base + g.R + b1;
+            const uintptr_t gs = ga & ~(uintptr_t)15;
+            uintptr_t cs = gs > A0 ? gs : A0;
+            uintptr_t ce = (ge + 15) & ~(uintptr_t)15;
+            if (ce > A1) ce = A1;
+            sm.pay_mis = (uint32_t)(ga - gs);
+            // bytes outside the 16-byte-aligned interior of the stream buffer
+            for (uintptr_t q = ga; q < ge && q < A0; q++) sm.pay[q - gs] = *reinterpret_cast<const uint8_t *>(q);
+            for (uintptr_t q = (ga > A1 ? ga : A1); q < ge; q++) sm.pay[q - gs] = *reinterpret_cast<const uint8_t *>(q);
+            fence_proxy_async_smem();
+            if (ce > cs) tx = (uint32_t)(ce - cs);
+            mbar_arrive_expect_tx(&sm.pay_full, tx);
+            if (tx) bulk_g2s(sm.pay + (cs - gs), reinterpret_cast<const void *>(cs), tx, &sm.pay_full);
+        } else {
+            mbar_arrive(&sm.pay_full);  // nothing valid to fetch; the checks below report it
+        }
+    }
     const TileInfo ti = tile_info(g, t);
     uint32_t n0;
     const unsigned long long row0 = brow_start(g, ti.rho0, n0);
@@ -1443,13 +1481,18 @@ __global__ void __launch_bounds__(kThreads, LSC_DEC_HOIST ? 3 : 4) dec_kernel(co
             if (g.R + base + agg > a.cap) {
                 raise_error(a.ctl, DEV_ERR_CAPACITY);
                 sm.flag_ok = 0;
+            } else if (a.tile_off[t + 1] != base + agg) {
+                raise_error(a.ctl, DEV_ERR_CORRUPT);
+                sm.flag_ok = 0;
             }
         }
     }
     __syncthreads();
-    if (!sm.flag_ok) return;
+    // the payload copy must land before the CTA returns or reads it
+    const bool landed = mbar_wait_landed(&sm.pay_full, 0);
+    if (!sm.flag_ok || !__syncthreads_and(landed)) return;
 
-    const uint8_t *const pay = a.in + g.R + sm.base;
+    const uint8_t *const pay = sm.pay + sm.pay_mis;
     const unsigned long long ebase = row0 * g.Z;  // element index of the tile's first row
     const uint32_t nunits = (ti.nblk + 7) >> 3;
 #if LSC_DEC_HOIST

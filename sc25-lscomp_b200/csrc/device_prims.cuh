@@ -118,6 +118,17 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, Launch
     return true;
 }
 
+// Wait, bounded by time only (not by the abort flag), for a phase whose
+// completion is a TMA load landing: used before a CTA releases shared
+// memory that a load may still be writing.  false if the limit passed.
+__device__ __forceinline__ bool mbar_wait_landed(uint64_t *bar, uint32_t parity)
+{
+    const unsigned long long t0 = global_ns();
+    while (!mbar_try_wait(bar, parity))
+        if (global_ns() - t0 > kWaitLimitNs) return false;
+    return true;
+}
+
 // ---------------------------------------------------------------- TMA bulk
 // 1-D bulk copy global -> shared, completion counted on an mbarrier.
 // dst, src 16-byte aligned; bytes a multiple of 16.
