@@ -445,6 +445,35 @@ __device__ __forceinline__ uint32_t max_all(const Row<uint32_t> &v)
     return m;
 }
 
+__device__ __forceinline__ uint32_t min2u16(uint32_t a, uint32_t b)
+{
+    uint32_t d;
+    asm("min.u16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+    return d;
+}
+
+// (w - B) mod 2^16 in each 16-bit half (no borrow between the halves)
+__device__ __forceinline__ uint32_t sub16x2(uint32_t w, uint32_t B)
+{
+    return ((w | 0x80008000u) - (B & 0x7fff7fffu)) ^ ((w ^ ~B) & 0x80008000u);
+}
+
+// per 16-bit half: min over the row of (v - b0) mod 2^16 (B = b0 in both halves)
+__device__ __forceinline__ uint32_t min16_from(const Row<uint16_t> &v, uint32_t B, uint32_t acc)
+{
+#pragma unroll
+    for (int i = 0; i < 4; i++) acc = min2u16(acc, sub16x2(v.w[i], B));
+    return acc;
+}
+
+// per 16-bit half: count of nonzero values of the row, added to acc
+__device__ __forceinline__ uint32_t nonzero16(const Row<uint16_t> &v, uint32_t acc)
+{
+#pragma unroll
+    for (int i = 0; i < 4; i++) acc += min2u16(v.w[i], 0x00010001u);
+    return acc;
+}
+
 // one value quantised by the chosen bin
 __device__ __forceinline__ uint32_t quant1(uint32_t v, const Codec &c, uint32_t choice, bool wide)
 {
@@ -856,11 +885,28 @@ __device__ __forceinline__ uint32_t block_header(const Row<T> &A, const Row<T> &
         // value lies between the two bins, so the choice is the interval
         // holding the smallest value >= bin0
         const uint32_t b0 = c.binc[0];
-        uint32_t mn = min_from(B, b0, min_from(A, b0, 0xffffffffu));
-        mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, 8));
-        mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, 16));
+        uint32_t mn;
+        bool any;
+        if constexpr (sizeof(T) == 2) {
+            // in 16-bit halves: the smallest (v - bin0) mod 2^16 over the block
+            // comes from a value >= bin0 when there is one, since every wrapped
+            // difference (v < bin0) is larger; bin0 > 65535 leaves none
+            if (b0 <= 0xffffu) {
+                const uint32_t m = min16_from(B, b0 * 0x10001u, min16_from(A, b0 * 0x10001u, 0xffffffffu));
+                mn = min(m & 0xffffu, m >> 16);
+            } else {
+                mn = 0xffffu;
+            }
+            mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, 8));
+            mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, 16));
+            any = b0 <= 0xffffu && mn <= 0xffffu - b0;
+        } else {
+            mn = min_from(B, b0, min_from(A, b0, 0xffffffffu));
+            mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, 8));
+            mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, 16));
+            any = mn <= ~b0;
+        }
         const uint32_t v = mn + b0;  // smallest value >= bin0 (if any)
-        const bool any = sizeof(T) == 2 ? (mn < 0x80000000u) : (mn <= ~b0);
         choice = (any && v < c.binc[1])   ? 0u
                  : (any && v < c.binc[2]) ? 1u
                  : (any && v < c.binc[3]) ? 2u
@@ -881,7 +927,13 @@ __device__ __forceinline__ uint32_t block_header(const Row<T> &A, const Row<T> &
     }
     bool pool = false;
     if (POOL) {
-        uint32_t zc = zeros(A) + zeros(B);
+        uint32_t zc;
+        if constexpr (sizeof(T) == 2) {
+            const uint32_t nz = nonzero16(B, nonzero16(A, 0u));
+            zc = 16u - ((nz & 0xffffu) + (nz >> 16));
+        } else {
+            zc = zeros(A) + zeros(B);
+        }
         zc += __shfl_xor_sync(0xffffffffu, zc, 8);
         zc += __shfl_xor_sync(0xffffffffu, zc, 16);
         pool = (int)zc >= c.pool_min;
@@ -889,12 +941,21 @@ __device__ __forceinline__ uint32_t block_header(const Row<T> &A, const Row<T> &
     // rate = bit length of the largest quantised value (cuLSZ_kernel.cu:937-957);
     // quantisation is monotone, so only the block maximum is divided
     uint32_t mx;
+    // (the pooled rows only when a block of the warp pools)
     if (IDENT) {
-        mx = pool ? or_all(pool_rows(A, B)) : (or_all(A) | or_all(B));  // same bit length as the max
+        mx = or_all(A) | or_all(B);  // same bit length as the max
+        if (POOL && __any_sync(0xffffffffu, pool)) {
+            const uint32_t mp = or_all(pool_rows(A, B));
+            if (pool) mx = mp;
+        }
         mx |= __shfl_xor_sync(0xffffffffu, mx, 8);
         mx |= __shfl_xor_sync(0xffffffffu, mx, 16);
     } else {
-        mx = pool ? max_all(pool_rows(A, B)) : max(max_all(A), max_all(B));
+        mx = max(max_all(A), max_all(B));
+        if (POOL && __any_sync(0xffffffffu, pool)) {
+            const uint32_t mp = max_all(pool_rows(A, B));
+            if (pool) mx = mp;
+        }
         mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, 8));
         mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, 16));
         mx = quant1(mx, c, choice, sizeof(T) == 4);
