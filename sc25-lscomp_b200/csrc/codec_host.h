@@ -192,9 +192,28 @@ inline int launch_enc_w(const EncArgs<T> &a, int sm_count, cudaStream_t st)
 }
 
 // Compute warps per encoder CTA: LSC_ENC_GROUPS groups of LSC_ENC_WPG warps.
+// Share of the compute warps' unit slots a tile fills when a group of wpg
+// warps takes its units round by round (8-block units, ceil(nblk / 8) of them).
+inline double unit_fill(const Geom &g, uint32_t wpg)
+{
+    const uint32_t nblk = g.chunked ? g.W : g.G * g.bzb;
+    const uint32_t units = (nblk + 7) / 8;
+    return (double)units / (double)(wpg * ((units + wpg - 1) / wpg));
+}
+
+// Shape of the encoder CTA.  The lossless uint16 kernel is bound by its
+// producer and writer warps and keeps LSC_ENC_GROUPS x LSC_ENC_WPG; the lossy
+// one is bound by its compute warps, and when groups of 7 warps fill a
+// tile's unit slots clearly better than groups of 8 (a block-row of 195
+// blocks: 25 units, 89% against 78%) it runs with 7 (measured on B200:
+// CSSI-like lossy compress 2.71 -> 2.59 ms; XPCS-like tiles of 32 units keep 8).
 template <typename T, int VEC, int BINS, bool POOL, bool BATCH>
 inline int launch_enc_t(const EncArgs<T> &a, int sm_count, cudaStream_t st)
 {
+    if constexpr (sizeof(T) == 2 && BINS != BINS_IDENT && !BATCH && LSC_ENC_GROUPS == 2 && LSC_ENC_WPG == 8) {
+        if (unit_fill(a.g, 7) > unit_fill(a.g, 8) + 0.05)
+            return launch_enc_w<T, VEC, BINS, POOL, 2, 7, BATCH>(a, sm_count, st);
+    }
     return launch_enc_w<T, VEC, BINS, POOL, LSC_ENC_GROUPS, LSC_ENC_WPG, BATCH>(a, sm_count, st);
 }
 
