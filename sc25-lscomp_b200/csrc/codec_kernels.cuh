@@ -41,6 +41,7 @@
 //                     1: 256-wide look-back bounded by the writer's previous tile
 //   LSC_DEC_HOIST     1: the decoder issues all payload loads of a warp's
 //                     units before transposing any of them
+//   LSC_DEC_CTAS      decoder CTAs per SM the register budget is sized for
 //   LSC_ENC_GROUPS    compute groups per encoder CTA (tiles in flight)
 //   LSC_ENC_WPG       warps per compute group
 #ifndef LSC_WRITERS
@@ -51,6 +52,9 @@
 #endif
 #ifndef LSC_DEC_HOIST
 #define LSC_DEC_HOIST 0
+#endif
+#ifndef LSC_DEC_CTAS
+#define LSC_DEC_CTAS 6  // decoder CTAs per SM the register budget is sized for (shared memory allows 6)
 #endif
 #ifndef LSC_ENC_GROUPS
 #define LSC_ENC_GROUPS 2  // independent compute groups per encoder CTA
@@ -1478,7 +1482,7 @@ __device__ __forceinline__ void dec_unit(const DecArgs<T> &a, const TileInfo &ti
 // (lsCOMP/src/cuLSZ_kernel.cu:1440-1640).  Every element of the tile is
 // written, zeros for blocks of rate 0.
 template <typename T, int VEC>
-__global__ void __launch_bounds__(kThreads, LSC_DEC_HOIST ? 3 : 4) dec_kernel(const DecArgs<T> a)
+__global__ void __launch_bounds__(kThreads, LSC_DEC_CTAS) dec_kernel(const DecArgs<T> a)
 {
     constexpr int NG = Elem<T>::kGroups;
     __shared__ DecSmem sm;
