@@ -1250,22 +1250,18 @@ __device__ __forceinline__ void enc_writer(const EncArgs<T> &a, EncSmem &sm, uin
             if (lane == 0) raise_error(a.ctl, DEV_ERR_CAPACITY);
             break;
         }
-        // copy [0, agg) of the ring slot to out + R + excl (4-byte aligned):
-        // 4-byte words up to the first 16-byte boundary, 16-byte stores after
+        // copy [0, agg) of the ring slot to out + R + excl (4-byte aligned)
         const uint8_t *src = sm.st[j];
         uint8_t *dst = out + g.R + excl;
-        uint32_t head = (uint32_t)((16u - ((uintptr_t)dst & 15u)) & 15u);
-        if (head > agg) head = agg;
-        if (lane < head / 4u) reinterpret_cast<uint32_t *>(dst)[lane] = reinterpret_cast<const uint32_t *>(src)[lane];
-        const uint32_t nbody = (agg - head) / 16u;
+        // in consecutive words per lane: conflict-free shared loads and 128
+        // contiguous bytes per warp store
+        {
+            const uint32_t *s32 = reinterpret_cast<const uint32_t *>(src);
+            uint32_t *d32 = reinterpret_cast<uint32_t *>(dst);
+            const uint32_t nw = agg / 4u;
 #pragma unroll 4
-        for (uint32_t c = lane; c < nbody; c += 32) {
-            const uint32_t *s4 = reinterpret_cast<const uint32_t *>(src + head + 16u * c);
-            *reinterpret_cast<uint4 *>(dst + head + 16u * c) = make_uint4(s4[0], s4[1], s4[2], s4[3]);
+            for (uint32_t w = lane; w < nw; w += 32) d32[w] = s32[w];
         }
-        const uint32_t tail = head + 16u * nbody;
-        if (lane < (agg - tail) / 4u)
-            reinterpret_cast<uint32_t *>(dst + tail)[lane] = reinterpret_cast<const uint32_t *>(src + tail)[lane];
         if (t == g.ntiles - 1) {
             if (lane == 0) {
                 if (BATCH) {
