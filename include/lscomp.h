@@ -218,6 +218,21 @@ int64_t lscomp_server_submit_decompress(lscomp_server *server, const void *h_con
 int lscomp_server_wait(lscomp_server *server, int64_t id, lscomp_server_result *result);
 int lscomp_server_stats(lscomp_server *server, uint64_t *rounds, uint64_t *batches, uint64_t *batched_requests);
 
+/* Lossy quality report on the GPU (the reference computes these on the host,
+   lsCOMP/src/cuLSZ_utility.cu:757-946 computePSNR / computeSSIM, on float
+   copies of the data; values are converted to float the same way).
+   psnr[6] (may be NULL): MSE, value range of the original, PSNR (dB), L2 norm
+   of the error, that norm over the L2 norm of the decoded data, NRMSE.
+   *ssim (may be NULL): mean SSIM over 7x7x7 windows placed every 2 elements
+   along each axis (NaN when a dimension is below 7).  Results equal the
+   host functions' up to the order of the final sums.  SSIM reads each value
+   ~170 times (about 1000x the cost of PSNR).  Allocates small partial-sum
+   buffers per call; synchronises the stream. */
+int lscomp_quality_u16(const uint16_t *d_ori, const uint16_t *d_dec, uint32_t x, uint32_t y, uint32_t z,
+                       double psnr[6], double *ssim, void *stream);
+int lscomp_quality_u32(const uint32_t *d_ori, const uint32_t *d_dec, uint32_t x, uint32_t y, uint32_t z,
+                       double psnr[6], double *ssim, void *stream);
+
 /* Wait for the workspace's last launch on `stream` and return its status. */
 int lscomp_workspace_check(lscomp_workspace *ws, void *stream);
 

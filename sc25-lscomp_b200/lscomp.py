@@ -124,6 +124,9 @@ def load_library() -> ctypes.CDLL:
     lib.lscomp_server_wait.argtypes = [vp, ctypes.c_int64, ctypes.POINTER(ServerResult)]
     lib.lscomp_server_stats.argtypes = [vp, pu64, pu64, pu64]
     for sfx in ("u16", "u32"):
+        getattr(lib, f"lscomp_quality_{sfx}").argtypes = [vp, vp, u32, u32, u32, ctypes.POINTER(ctypes.c_double),
+                                                          ctypes.POINTER(ctypes.c_double), vp]
+    for sfx in ("u16", "u32"):
         getattr(lib, f"lscomp_compress_batch_{sfx}").argtypes = [vp, ctypes.POINTER(LscompStack), u32, bins_t, f32,
                                                                  pu64, pu64, vp]
     _lib = lib
@@ -340,6 +343,23 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def quality(d_ori, d_dec, dims, ssim: bool = True, stream=None) -> dict:
+    """PSNR report and (optionally) the 7x7x7 SSIM of an original stack and its
+    decoded copy, on the GPU (lscomp_quality_*): the reference's computePSNR /
+    computeSSIM definitions on float copies of the values."""
+    lib = load_library()
+    x, y, z = (int(v) for v in dims)
+    p = (ctypes.c_double * 6)()
+    sv = ctypes.c_double(0.0)
+    _check(getattr(lib, f"lscomp_quality_{_suffix(d_ori)}")(
+        ctypes.c_void_p(d_ori.data_ptr()), ctypes.c_void_p(d_dec.data_ptr()), x, y, z, p,
+        ctypes.byref(sv) if ssim else None, ctypes.c_void_p(_stream_handle(stream))), f"lscomp_quality_{_suffix(d_ori)}")
+    out = {"mse": p[0], "range": p[1], "psnr": p[2], "l2_error": p[3], "l2_error_rel": p[4], "nrmse": p[5]}
+    if ssim:
+        out["ssim"] = sv.value
+    return out
 
 
 def compress_async(ws: Workspace, d_in, dims, bins, pooling: float, d_out, d_sizes=None, stream=None):
