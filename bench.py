@@ -327,6 +327,10 @@ def bench_batch(args, local):
             assert lscomp.compress_into(ws, d_in, dims, bins, p, chk) == (sl, rs)
             assert torch.equal(chk[:sl], d_out[:sl]), "batch stream differs from the single-stack stream"
         t_batch = timed(lambda: lscomp.compress_batch(ws, items, bins, p), args.steps)
+        plan = lscomp.Plan(ws, items, bins, p)
+        assert plan.run() == got, "graph plan sizes differ from the batch call"
+        t_plan = timed(plan.run, args.steps)
+        plan.close()
 
         def loop_async():
             for d_in, dims, d_out in items:
@@ -338,15 +342,32 @@ def bench_batch(args, local):
 
         t_async = timed(loop_async, args.steps)
         t_sync = timed(loop_sync, args.steps)
-        res[name] = {"batch_ms": round(t_batch, 3), "per_stack_async_ms": round(t_async, 3),
+        res[name] = {"batch_ms": round(t_batch, 3), "graph_plan_ms": round(t_plan, 3),
+                     "graph_plan_frames_per_s": round(frames / t_plan * 1e3, 1),
+                     "per_stack_async_ms": round(t_async, 3),
                      "per_stack_sync_ms": round(t_sync, 3), "frames_per_s": round(frames / t_batch * 1e3, 1),
                      "input_gbs": round(nbytes / t_batch / 1e6, 1),
                      "speedup_vs_per_stack_async": round(t_async / t_batch, 2),
                      "speedup_vs_per_stack_sync": round(t_sync / t_batch, 2)}
     print(json.dumps({"metric": "batched compress frames per second (one lscomp_compress_batch_u16 call)",
                       "value": res["lossless"]["frames_per_s"], "unit": "frames/s", "higher_is_better": True,
-                      "per_mode": res, "config": config, "timing": "CUDA events around each call, median of "
-                      f"{args.steps}; sizes read back to the host inside the batch call"}))
+                      "per_mode": res, "config": config, "tuned": tuned_summary(lscomp, ("batch",)),
+                      "timing": "CUDA events around each call, median of "
+                      f"{args.steps}; sizes read back to the host inside the batch call and the graph replay"}))
+
+
+def tuned_summary(lscomp, kinds=("compress", "batch", "decompress")):
+    """The tuner's choices so far: key -> chosen shape/tile size and the
+    candidates' measured ms per call."""
+    shapes = {-1: "rule", 0: "2x8", 1: "2x7"}
+    out = []
+    for e in lscomp.tune_table():
+        if e["kind"] not in kinds:
+            continue
+        out.append({"kind": e["kind"], "es": e["es"], "layout": e["layout"], "pool": e["pool"], "bzb": e["bzb"],
+                    "chosen": f"{shapes[e['shape']]}/{e['tile_blocks']}",
+                    "ms": {f"{shapes[t['shape']]}/{t['tile_blocks']}": t["ms"] for t in e["times"]}})
+    return out
 
 
 def bench_serve(args, local):
@@ -557,7 +578,7 @@ def main():
            "warmup": max(args.warmup, 3), "ms_per_step": round(ms_step, 4), "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic (seeded CSSI-like generator)",
            "config": config, "per_mode": per, "roofline": roofline, "e2e": e2e, "gpu_launches": int(launches),
-           "clocks": clk}
+           "clocks": clk, "tuned": tuned_summary(lscomp)}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args.kind, dims, args.cpu_seconds)
     if rank == 0:

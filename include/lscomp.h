@@ -153,6 +153,62 @@ int lscomp_compress_batch_u32(lscomp_workspace *ws, const lscomp_stack *stacks, 
                               const uint32_t bins[4], float pooling, uint64_t *stream_len,
                               uint64_t *ref_size, void *stream);
 
+/* Graph plans (no counterpart in the reference).  A plan fixes one
+   compression -- n stacks (n = 1: the single-stack kernel, n > 1: the batch
+   kernel), their buffers and shapes, bins and pooling threshold -- and
+   captures it once as a CUDA graph: clearing the scan state, the encoder
+   launch and the copy of the sizes and the status to pinned host memory.
+   lscomp_plan_run replays the graph on `stream`, waits for it and returns
+   the status and the sizes as lscomp_compress_batch_* does; nothing is
+   computed or copied on the host per call beyond that.  For loops that
+   compress new contents of the same buffers again and again (acquisition
+   frames landing in fixed device buffers).  Create runs one ordinary call
+   through `ws` first (argument checks, tuning when on; the streams are
+   written), then allocates the plan's own scratch (about 12 bytes per tile
+   plus the stack table), so plans and workspace calls never share state.
+   Replays of one plan are serialised; different plans may run
+   concurrently. */
+typedef struct lscomp_plan lscomp_plan;
+int lscomp_plan_create_u16(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, const uint32_t bins[4],
+                           float pooling, void *stream, lscomp_plan **plan);
+int lscomp_plan_create_u32(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, const uint32_t bins[4],
+                           float pooling, void *stream, lscomp_plan **plan);
+int lscomp_plan_run(lscomp_plan *plan, void *stream, uint64_t *stream_len, uint64_t *ref_size);
+int lscomp_plan_destroy(lscomp_plan *plan);
+
+/* Launch-configuration tuner (no counterpart in the reference, whose launch
+   shape is fixed).  A configuration is the encoder CTA shape (2 groups of 8
+   or of 7 compute warps) and the most 8x8 blocks a tile holds (uint16: 256
+   or 128; uint32: 128 or 64); the decoder only has the tile size.  Every
+   configuration writes the same stream.  With tuning on (the default;
+   environment LSCOMP_AUTOTUNE=0 or lscomp_tune_mode(0) turns it off) the
+   first compress / decompress / batch call of a key -- element type, bins
+   layout (lossless, equal, increasing, other), pooling on or off, row
+   access width, blocks per block-row (single stacks) -- times every
+   candidate on the call's own buffers (one untimed and three timed calls
+   each, CUDA events) and keeps the fastest for the process; that first
+   call therefore synchronises its stream and takes about 16x as long.
+   With tuning off, or while the stream is being captured, keys not in the
+   table use built-in rules.  lscomp_compress_u16_noalloc uses the table
+   but never tunes.
+   lscomp_tune_mode: 0 off, 1 on, other values only query; returns the
+   previous mode.  lscomp_tune_report writes the table as text (one line per
+   key: "es layout pool kind vec bzb -> shape tile_blocks", then
+   " | shape tile_blocks ms" per timed candidate; kind 0 compress, 1 batch,
+   2 decompress; shape -1 = rule, 0 = 2x8, 1 = 2x7) and returns the bytes
+   needed including the terminating NUL.  lscomp_tune_save / _load write and
+   read that text (load replaces the keys it names; a malformed file changes
+   nothing and returns LSCOMP_ERR_ARG).  Single stacks of fewer than 4
+   tiles per SM (about 150,000 8x8 blocks of uint16 on B200) are never
+   tuned: they use the table or the rules.  lscomp_tune_hits counts the
+   calls that found their key in the table. */
+int lscomp_tune_mode(int mode);
+uint64_t lscomp_tune_hits(void);
+int lscomp_tune_clear(void);
+uint64_t lscomp_tune_report(char *buf, uint64_t cap);
+int lscomp_tune_save(const char *path);
+int lscomp_tune_load(const char *path);
+
 /* Container (no counterpart in the reference, whose streams carry neither
    dimensions, bins, pooling threshold nor element type, and whose size is
    returned out of band).  A container is a 64-byte header -- magic "LSCZ",

@@ -25,18 +25,27 @@ int compress_async_t(lscomp_workspace *ws, const T *d_in, uint32_t x, uint32_t y
     if (!ws || !d_in || !d_out) return LSCOMP_ERR_ARG;
     // the stream is written in 4-byte words
     if (reinterpret_cast<uintptr_t>(d_in) % sizeof(T) || reinterpret_cast<uintptr_t>(d_out) % 4u) return LSCOMP_ERR_ARG;
-    EncArgs<T> a;
+    Geom g0;
+    Codec c;
     int layout = 0;
-    if (!make_geom(x, y, z, Elem<T>::kTileBlocks, a.g) || !make_codec(bins, pooling, sizeof(T) == 4, a.c, layout))
+    if (!make_geom(x, y, z, Elem<T>::kTileBlocks, g0) || !make_codec(bins, pooling, sizeof(T) == 4, c, layout))
         return LSCOMP_ERR_ARG;
-    if (cap < a.g.R) return LSCOMP_ERR_CAPACITY;
+    if (cap < g0.R) return LSCOMP_ERR_CAPACITY;
+    const int vec = vec_class(d_in, z, sizeof(T));
+    if (sizeof(T) == 4 && vec == 2) return LSCOMP_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
     std::lock_guard<std::mutex> lk(ws->mu);
     int prev = 0;
     cudaGetDevice(&prev);
     if (prev != ws->device) cudaSetDevice(ws->device);
-    int s = ws_prepare(ws, a.g.ntiles, st);
-    if (!s) {
+    const bool pool = c.pool_min <= 64;
+    // one complete call with configuration cfg (the tuner runs it too)
+    auto run = [&](const TuneCfg &cfg) -> int {
+        EncArgs<T> a = {};
+        make_geom(x, y, z, cfg.tile_blocks, a.g);
+        int s = ws_prepare(ws, a.g.ntiles, st);
+        if (s) return s;
+        a.c = c;
         a.in = d_in;
         a.out = d_out;
         a.cap = cap;
@@ -44,16 +53,12 @@ int compress_async_t(lscomp_workspace *ws, const T *d_in, uint32_t x, uint32_t y
         a.state = ws->state;
         a.epoch = ws->epoch;
         a.sizes_out = reinterpret_cast<unsigned long long *>(d_sizes);
-        const bool pool = a.c.pool_min <= 64;
-        switch (vec_class(d_in, z, sizeof(T))) {
-        case 16: s = launch_enc_v<T, 16, false>(a, layout, pool, ws->sm_count, st); break;
-        case 4: s = launch_enc_v<T, 4, false>(a, layout, pool, ws->sm_count, st); break;
-        default:
-            if (sizeof(T) == 2) s = launch_enc_v<T, 2, false>(a, layout, pool, ws->sm_count, st);
-            else s = LSCOMP_ERR_ARG;
-            break;
-        }
-    }
+        return launch_enc_any<T, false>(a, vec, layout, pool, cfg.shape, ws->sm_count, st);
+    };
+    const TuneKey key{(uint8_t)sizeof(T), (uint8_t)layout, (uint8_t)pool, kTuneCompress, (uint8_t)vec, g0.bzb};
+    const bool may_tune = g0.ntiles >= (uint64_t)kTuneMinTilesPerSm * ws->sm_count;
+    const TuneCfg cfg = tune_choose(ws, key, TuneCfg{-1, (uint32_t)Elem<T>::kTileBlocks}, may_tune, st, run);
+    const int s = run(cfg);
     if (prev != ws->device) cudaSetDevice(prev);
     return s;
 }
@@ -83,18 +88,25 @@ int decompress_async_t(lscomp_workspace *ws, const uint8_t *d_in, uint64_t cmp_l
     if (!ws || !d_in || !d_out) return LSCOMP_ERR_ARG;
     // the stream is read in 4-byte words
     if (reinterpret_cast<uintptr_t>(d_out) % sizeof(T) || reinterpret_cast<uintptr_t>(d_in) % 4u) return LSCOMP_ERR_ARG;
-    DecArgs<T> a;
+    Geom g0;
+    Codec c;
     int layout = 0;
-    if (!make_geom(x, y, z, Elem<T>::kTileBlocks, a.g) || !make_codec(bins, pooling, sizeof(T) == 4, a.c, layout))
+    if (!make_geom(x, y, z, Elem<T>::kTileBlocks, g0) || !make_codec(bins, pooling, sizeof(T) == 4, c, layout))
         return LSCOMP_ERR_ARG;
-    if (cmp_len < a.g.nb) return LSCOMP_ERR_CAPACITY;
+    if (cmp_len < g0.nb) return LSCOMP_ERR_CAPACITY;
+    const int vec = vec_class(d_out, z, sizeof(T));
+    if (sizeof(T) == 4 && vec == 2) return LSCOMP_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
     std::lock_guard<std::mutex> lk(ws->mu);
     int prev = 0;
     cudaGetDevice(&prev);
     if (prev != ws->device) cudaSetDevice(ws->device);
-    int s = ws_prepare(ws, a.g.ntiles, st);
-    if (!s) {
+    auto run = [&](const TuneCfg &cfg) -> int {
+        DecArgs<T> a = {};
+        make_geom(x, y, z, cfg.tile_blocks, a.g);
+        int s = ws_prepare(ws, a.g.ntiles, st);
+        if (s) return s;
+        a.c = c;
         a.in = d_in;
         a.out = d_out;
         a.cap = cmp_len;
@@ -102,15 +114,19 @@ int decompress_async_t(lscomp_workspace *ws, const uint8_t *d_in, uint64_t cmp_l
         a.state = ws->state;
         a.tile_off = ws->state + ws->state_cap;
         a.epoch = ws->epoch;
-        switch (vec_class(d_out, z, sizeof(T))) {
-        case 16: s = launch_dec_t<T, 16>(a, ws->sm_count, st); break;
-        case 4: s = launch_dec_t<T, 4>(a, ws->sm_count, st); break;
+        switch (vec) {
+        case 16: return launch_dec_t<T, 16>(a, ws->sm_count, st);
+        case 4: return launch_dec_t<T, 4>(a, ws->sm_count, st);
         default:
-            if (sizeof(T) == 2) s = launch_dec_t<T, 2>(a, ws->sm_count, st);
-            else s = LSCOMP_ERR_ARG;
-            break;
+            if constexpr (sizeof(T) == 2) return launch_dec_t<T, 2>(a, ws->sm_count, st);
+            return LSCOMP_ERR_ARG;
         }
-    }
+    };
+    const TuneKey key{(uint8_t)sizeof(T), (uint8_t)layout, (uint8_t)(c.pool_min <= 64), kTuneDecompress, (uint8_t)vec,
+                      g0.bzb};
+    const bool may_tune = g0.ntiles >= (uint64_t)kTuneMinTilesPerSm * ws->sm_count;
+    const TuneCfg cfg = tune_choose(ws, key, TuneCfg{-1, (uint32_t)Elem<T>::kTileBlocks}, may_tune, st, run);
+    const int s = run(cfg);
     if (prev != ws->device) cudaSetDevice(prev);
     return s;
 }
@@ -327,6 +343,20 @@ extern "C" int lscomp_compress_u16_noalloc(const uint16_t *d_in, uint32_t x, uin
     if (!make_geom(x, y, z, Elem<uint16_t>::kTileBlocks, a.g) || !make_codec(bins, pooling, false, a.c, layout))
         return LSCOMP_ERR_ARG;
     if (a.g.ntiles > kNoAllocMaxTiles) return LSCOMP_ERR_TOO_LARGE;
+    const bool pool = a.c.pool_min <= 64;
+    const int vec = vec_class(d_in, z, 2);
+    // a configuration the tuner chose for this key earlier is used when its
+    // tiles fit the scratch area; no tuning runs here
+    TuneCfg cfg{-1, (uint32_t)Elem<uint16_t>::kTileBlocks};
+    {
+        TuneCfg t;
+        Geom gt;
+        const TuneKey key{2, (uint8_t)layout, (uint8_t)pool, kTuneCompress, (uint8_t)vec, a.g.bzb};
+        if (tune_lookup(key, t) && make_geom(x, y, z, t.tile_blocks, gt) && gt.ntiles <= kNoAllocMaxTiles) {
+            cfg = t;
+            a.g = gt;
+        }
+    }
     if (cap < a.g.R) return LSCOMP_ERR_CAPACITY;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) return LSCOMP_ERR_CUDA;
@@ -362,13 +392,7 @@ extern "C" int lscomp_compress_u16_noalloc(const uint16_t *d_in, uint32_t x, uin
     a.state = state;
     a.epoch = d.epoch;
     a.sizes_out = nullptr;
-    const bool pool = a.c.pool_min <= 64;
-    int s;
-    switch (vec_class(d_in, z, 2)) {
-    case 16: s = launch_enc_v<uint16_t, 16, false>(a, layout, pool, d.sm_count, st); break;
-    case 4: s = launch_enc_v<uint16_t, 4, false>(a, layout, pool, d.sm_count, st); break;
-    default: s = launch_enc_v<uint16_t, 2, false>(a, layout, pool, d.sm_count, st); break;
-    }
+    int s = launch_enc_any<uint16_t, false>(a, vec, layout, pool, cfg.shape, d.sm_count, st);
     if (s) return s;
     LaunchCtl h;  // plain host memory: the copy allocates nothing
     e = cudaMemcpyAsync(&h, d.scratch, sizeof(LaunchCtl), cudaMemcpyDeviceToHost, st);

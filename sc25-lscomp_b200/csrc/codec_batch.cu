@@ -9,6 +9,7 @@
 // once, so no look-back walk crosses into the previous stack.  Each stack's
 // stream is exactly the one lscomp_compress_u16/_u32 writes for it alone.
 #include <string.h>
+#include <mutex>
 #include <vector>
 #include "codec_host.h"
 
@@ -63,6 +64,22 @@ int batch_reserve(lscomp_workspace *ws, uint32_t n, uint64_t ntiles, cudaStream_
     return LSCOMP_OK;
 }
 
+// Per-stack geometry with tiles of at most tile_blocks blocks and each
+// stack's first tile over the batch; false if a stack's dims are invalid.
+inline bool batch_geoms(const lscomp_stack *stacks, uint32_t n, uint32_t tile_blocks, std::vector<Geom> &geom,
+                        std::vector<unsigned long long> &tile0, unsigned long long &total)
+{
+    geom.resize(n);
+    tile0.resize(n);
+    total = 0;
+    for (uint32_t s = 0; s < n; s++) {
+        if (!make_geom(stacks[s].x, stacks[s].y, stacks[s].z, tile_blocks, geom[s])) return false;
+        tile0[s] = total;
+        total += geom[s].ntiles;
+    }
+    return true;
+}
+
 template <typename T>
 int compress_batch_t(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, const uint32_t bins[4],
                      float pooling, uint64_t *stream_len, uint64_t *ref_size, void *stream)
@@ -74,8 +91,8 @@ int compress_batch_t(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t 
     if (!make_codec(bins, pooling, sizeof(T) == 4, c, layout)) return LSCOMP_ERR_ARG;
     // every stack checked as lscomp_compress_* checks it; the narrowest
     // row access any stack allows is used for all
-    std::vector<Geom> geom(n);
-    std::vector<unsigned long long> tile0(n);
+    std::vector<Geom> geom;
+    std::vector<unsigned long long> tile0;
     unsigned long long total = 0;
     int vec = 16;
     for (uint32_t s = 0; s < n; s++) {
@@ -83,12 +100,11 @@ int compress_batch_t(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t 
         if (!q.d_in || !q.d_out) return LSCOMP_ERR_ARG;
         if (reinterpret_cast<uintptr_t>(q.d_in) % sizeof(T) || reinterpret_cast<uintptr_t>(q.d_out) % 4u)
             return LSCOMP_ERR_ARG;
-        if (!make_geom(q.x, q.y, q.z, Elem<T>::kTileBlocks, geom[s])) return LSCOMP_ERR_ARG;
-        if (q.cap < geom[s].R) return LSCOMP_ERR_CAPACITY;
+        Geom g;
+        if (!make_geom(q.x, q.y, q.z, Elem<T>::kTileBlocks, g)) return LSCOMP_ERR_ARG;
+        if (q.cap < g.R) return LSCOMP_ERR_CAPACITY;
         const int v = vec_class(q.d_in, q.z, sizeof(T));
         if (v < vec) vec = v;
-        tile0[s] = total;
-        total += geom[s].ntiles;
     }
     if (sizeof(T) == 4 && vec == 2) return LSCOMP_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
@@ -96,27 +112,39 @@ int compress_batch_t(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t 
     int prev = 0;
     cudaGetDevice(&prev);
     if (prev != ws->device) cudaSetDevice(ws->device);
-    int r = ws_prepare(ws, total, st);
-    if (!r) r = batch_reserve(ws, n, total, st);
-    if (!r) {
-        for (uint32_t s = 0; s < n; s++) {
-            BatchStack &b = ws->h_stacks[s];
-            b.g = geom[s];
-            b.in = stacks[s].d_in;
-            b.out = stacks[s].d_out;
-            b.cap = stacks[s].cap;
-            b.tile0 = tile0[s];
-            b.sizes = ws->d_bsizes + 2ull * s;
+    const bool pool = c.pool_min <= 64;
+    // one complete call with configuration cfg.  The descriptors are rebuilt
+    // only when the tile size changes; the tuner synchronises the stream
+    // before it changes configuration, so no pending copy reads the pinned
+    // descriptors while they are rewritten.
+    uint32_t built = 0;
+    auto run = [&](const TuneCfg &cfg) -> int {
+        int r = LSCOMP_OK;
+        if (cfg.tile_blocks != built) {
+            if (!batch_geoms(stacks, n, cfg.tile_blocks, geom, tile0, total)) return LSCOMP_ERR_ARG;
+            r = batch_reserve(ws, n, total, st);
+            if (r) return r;
+            for (uint32_t s = 0; s < n; s++) {
+                BatchStack &b = ws->h_stacks[s];
+                b.g = geom[s];
+                b.in = stacks[s].d_in;
+                b.out = stacks[s].d_out;
+                b.cap = stacks[s].cap;
+                b.tile0 = tile0[s];
+                b.sizes = ws->d_bsizes + 2ull * s;
+            }
+            r = cuda_status(
+                cudaMemcpyAsync(ws->d_stacks, ws->h_stacks, n * sizeof(BatchStack), cudaMemcpyHostToDevice, st));
+            if (r) return r;
+            const uint32_t grid = n < 4096u ? n : 4096u;
+            tile_stack_kernel<<<grid, 256, 0, st>>>(ws->d_stacks, n, ws->d_tile_stack);
+            g_launches.fetch_add(1);
+            r = cuda_status(cudaGetLastError());
+            if (r) return r;
+            built = cfg.tile_blocks;
         }
-        r = cuda_status(cudaMemcpyAsync(ws->d_stacks, ws->h_stacks, n * sizeof(BatchStack), cudaMemcpyHostToDevice, st));
-    }
-    if (!r) {
-        const uint32_t grid = n < 4096u ? n : 4096u;
-        tile_stack_kernel<<<grid, 256, 0, st>>>(ws->d_stacks, n, ws->d_tile_stack);
-        g_launches.fetch_add(1);
-        r = cuda_status(cudaGetLastError());
-    }
-    if (!r) {
+        r = ws_prepare(ws, total, st);
+        if (r) return r;
         EncArgs<T> a;
         memset(&a, 0, sizeof(a));
         a.g = geom[0];  // not read by batch launches
@@ -127,16 +155,11 @@ int compress_batch_t(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t 
         a.stacks = ws->d_stacks;
         a.tile_stack = ws->d_tile_stack;
         a.ntiles_all = total;
-        const bool pool = c.pool_min <= 64;
-        switch (vec) {
-        case 16: r = launch_enc_v<T, 16, true>(a, layout, pool, ws->sm_count, st); break;
-        case 4: r = launch_enc_v<T, 4, true>(a, layout, pool, ws->sm_count, st); break;
-        default:
-            if (sizeof(T) == 2) r = launch_enc_v<T, 2, true>(a, layout, pool, ws->sm_count, st);
-            else r = LSCOMP_ERR_ARG;
-            break;
-        }
-    }
+        return launch_enc_any<T, true>(a, vec, layout, pool, cfg.shape, ws->sm_count, st);
+    };
+    const TuneKey key{(uint8_t)sizeof(T), (uint8_t)layout, (uint8_t)pool, kTuneBatch, (uint8_t)vec, 0};
+    const TuneCfg cfg = tune_choose(ws, key, TuneCfg{-1, (uint32_t)Elem<T>::kTileBlocks}, true, st, run);
+    int r = run(cfg);
     if (!r)
         r = cuda_status(cudaMemcpyAsync(ws->h_bsizes, ws->d_bsizes, 2ull * n * sizeof(unsigned long long),
                                         cudaMemcpyDeviceToHost, st));
@@ -150,6 +173,211 @@ int compress_batch_t(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t 
         }
     }
     if (prev != ws->device) cudaSetDevice(prev);
+    return r;
+}
+
+// the single-stack asynchronous call for one stack descriptor
+template <typename T>
+int compress_async_t_dispatch(lscomp_workspace *ws, const lscomp_stack &q, const uint32_t bins[4], float pooling,
+                              void *stream)
+{
+    if constexpr (sizeof(T) == 2)
+        return lscomp_compress_u16_async(ws, static_cast<const uint16_t *>(q.d_in), q.x, q.y, q.z, bins, pooling,
+                                         q.d_out, q.cap, nullptr, stream);
+    else
+        return lscomp_compress_u32_async(ws, static_cast<const uint32_t *>(q.d_in), q.x, q.y, q.z, bins, pooling,
+                                         q.d_out, q.cap, nullptr, stream);
+}
+
+// ---------------------------------------------------------------- graph plans
+// A plan is one batch compression with everything fixed (the stacks'
+// buffers and shapes, bins, pooling threshold, launch configuration),
+// captured once as a CUDA graph: clear the control block and the look-back
+// words, run the encoder, copy the per-stack sizes and the control block to
+// pinned host memory.  A replay is one graph launch and one synchronisation;
+// the host computes nothing per call.  The plan owns its scratch (look-back
+// words at a fixed epoch, cleared by the graph itself), so plans and
+// workspace calls do not share state.
+struct PlanImpl {
+    std::mutex mu;
+    int device = 0;
+    int es = 2;
+    uint32_t n = 0;
+    TuneCfg cfg{-1, 0};
+    uint64_t ntiles = 0;
+    std::vector<uint64_t> nb;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    LaunchCtl *ctl = nullptr, *h_ctl = nullptr;
+    unsigned long long *state = nullptr;
+    BatchStack *d_stacks = nullptr;
+    uint32_t *d_tile_stack = nullptr;
+    unsigned long long *d_sizes = nullptr, *h_sizes = nullptr;
+};
+
+void plan_free(PlanImpl *p)
+{
+    if (!p) return;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(p->device);
+    if (p->exec) cudaGraphExecDestroy(p->exec);
+    if (p->graph) cudaGraphDestroy(p->graph);
+    if (p->ctl) cudaFree(p->ctl);
+    if (p->h_ctl) cudaFreeHost(p->h_ctl);
+    if (p->state) cudaFree(p->state);
+    if (p->d_stacks) cudaFree(p->d_stacks);
+    if (p->d_tile_stack) cudaFree(p->d_tile_stack);
+    if (p->d_sizes) cudaFree(p->d_sizes);
+    if (p->h_sizes) cudaFreeHost(p->h_sizes);
+    cudaSetDevice(prev);
+    delete p;
+}
+
+constexpr uint32_t kPlanEpoch = 1;  // the graph clears the look-back words before every replay
+
+template <typename T>
+int plan_create_t(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, const uint32_t bins[4],
+                  float pooling, void *stream, PlanImpl **out)
+{
+    if (!out) return LSCOMP_ERR_ARG;
+    *out = nullptr;
+    if (!ws || !stacks || n == 0) return LSCOMP_ERR_ARG;
+    // one ordinary call first: it checks every argument, tunes the key when
+    // tuning is on, and leaves the streams written
+    int r = n == 1 ? compress_async_t_dispatch<T>(ws, stacks[0], bins, pooling, stream)
+                   : compress_batch_t<T>(ws, stacks, n, bins, pooling, nullptr, nullptr, stream);
+    if (!r && n == 1) r = lscomp_workspace_check(ws, stream);
+    if (r) return r;
+    Codec c;
+    int layout = 0;
+    make_codec(bins, pooling, sizeof(T) == 4, c, layout);
+    const bool pool = c.pool_min <= 64;
+    int vec = 16;
+    for (uint32_t s = 0; s < n; s++) {
+        const int v = vec_class(stacks[s].d_in, stacks[s].z, sizeof(T));
+        if (v < vec) vec = v;
+    }
+    Geom g0;
+    make_geom(stacks[0].x, stacks[0].y, stacks[0].z, Elem<T>::kTileBlocks, g0);
+    TuneCfg cfg{-1, (uint32_t)Elem<T>::kTileBlocks};
+    const TuneKey key{(uint8_t)sizeof(T), (uint8_t)layout, (uint8_t)pool, n == 1 ? kTuneCompress : kTuneBatch,
+                      (uint8_t)vec, n == 1 ? g0.bzb : 0u};
+    tune_lookup(key, cfg);
+
+    PlanImpl *p = new (std::nothrow) PlanImpl();
+    if (!p) return LSCOMP_ERR_NOMEM;
+    p->device = ws->device;
+    p->es = (int)sizeof(T);
+    p->n = n;
+    p->cfg = cfg;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(p->device);
+    std::vector<Geom> geom;
+    std::vector<unsigned long long> tile0;
+    unsigned long long total = 0;
+    batch_geoms(stacks, n, cfg.tile_blocks, geom, tile0, total);
+    p->ntiles = total;
+    p->nb.resize(n);
+    for (uint32_t s = 0; s < n; s++) p->nb[s] = geom[s].nb;
+    cudaStream_t cs = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&p->ctl, sizeof(LaunchCtl));
+    if (e == cudaSuccess) e = cudaMallocHost(&p->h_ctl, sizeof(LaunchCtl));
+    if (e == cudaSuccess) e = cudaMalloc(&p->state, total * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_sizes, 2ull * n * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMallocHost(&p->h_sizes, 2ull * n * sizeof(unsigned long long));
+    if (e == cudaSuccess && n > 1) {
+        std::vector<BatchStack> h(n);
+        for (uint32_t s = 0; s < n; s++) {
+            h[s].g = geom[s];
+            h[s].in = stacks[s].d_in;
+            h[s].out = stacks[s].d_out;
+            h[s].cap = stacks[s].cap;
+            h[s].tile0 = tile0[s];
+            h[s].sizes = p->d_sizes + 2ull * s;
+        }
+        e = cudaMalloc(&p->d_stacks, n * sizeof(BatchStack));
+        if (e == cudaSuccess) e = cudaMalloc(&p->d_tile_stack, total * sizeof(uint32_t));
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(p->d_stacks, h.data(), n * sizeof(BatchStack), cudaMemcpyHostToDevice, cs);
+        if (e == cudaSuccess) {
+            const uint32_t grid = n < 4096u ? n : 4096u;
+            tile_stack_kernel<<<grid, 256, 0, cs>>>(p->d_stacks, n, p->d_tile_stack);
+            g_launches.fetch_add(1);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(cs);
+    }
+    r = cuda_status(e);
+    if (!r) {
+        EncArgs<T> a;
+        memset(&a, 0, sizeof(a));
+        a.g = geom[0];
+        a.c = c;
+        a.ctl = p->ctl;
+        a.state = p->state;
+        a.epoch = kPlanEpoch;
+        if (n == 1) {
+            a.in = static_cast<const T *>(stacks[0].d_in);
+            a.out = stacks[0].d_out;
+            a.cap = stacks[0].cap;
+            a.sizes_out = p->d_sizes;
+        } else {
+            a.stacks = p->d_stacks;
+            a.tile_stack = p->d_tile_stack;
+            a.ntiles_all = total;
+        }
+        e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed);
+        if (e == cudaSuccess) {
+            cudaMemsetAsync(p->ctl, 0, sizeof(LaunchCtl), cs);
+            cudaMemsetAsync(p->state, 0, total * sizeof(unsigned long long), cs);
+            const int lr = n == 1 ? launch_enc_any<T, false>(a, vec, layout, pool, cfg.shape, ws->sm_count, cs)
+                                  : launch_enc_any<T, true>(a, vec, layout, pool, cfg.shape, ws->sm_count, cs);
+            cudaMemcpyAsync(p->h_sizes, p->d_sizes, 2ull * n * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                            cs);
+            cudaMemcpyAsync(p->h_ctl, p->ctl, sizeof(LaunchCtl), cudaMemcpyDeviceToHost, cs);
+            e = cudaStreamEndCapture(cs, &p->graph);
+            if (e == cudaSuccess && lr) e = cudaErrorLaunchFailure;
+        }
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&p->exec, p->graph, 0);
+        r = cuda_status(e);
+    }
+    if (cs) cudaStreamDestroy(cs);
+    cudaSetDevice(prev);
+    if (r) {
+        plan_free(p);
+        return r;
+    }
+    *out = p;
+    return LSCOMP_OK;
+}
+
+int plan_run(PlanImpl *p, void *stream, uint64_t *stream_len, uint64_t *ref_size)
+{
+    if (!p) return LSCOMP_ERR_ARG;
+    std::lock_guard<std::mutex> lk(p->mu);
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (prev != p->device) cudaSetDevice(p->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e = cudaGraphLaunch(p->exec, st);
+    if (e == cudaSuccess) {
+        g_launches.fetch_add(1);
+        e = cudaStreamSynchronize(st);
+    }
+    int r = cuda_status(e);
+    if (!r) r = dev_status(p->h_ctl->error);
+    if (!r) {
+        for (uint32_t s = 0; s < p->n; s++) {
+            uint64_t total_s = p->h_sizes[2ull * s + 1];
+            if (p->es == 4) total_s &= 0xffffffffull;  // the reference reports a 32-bit total for uint32
+            if (stream_len) stream_len[s] = p->h_sizes[2ull * s];
+            if (ref_size) ref_size[s] = total_s + p->nb[s];
+        }
+    }
+    if (prev != p->device) cudaSetDevice(prev);
     return r;
 }
 
@@ -167,6 +395,29 @@ int lscomp_compress_batch_u32(lscomp_workspace *ws, const lscomp_stack *stacks, 
                               float pooling, uint64_t *stream_len, uint64_t *ref_size, void *stream)
 {
     return compress_batch_t<uint32_t>(ws, stacks, n, bins, pooling, stream_len, ref_size, stream);
+}
+
+int lscomp_plan_create_u16(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, const uint32_t bins[4],
+                           float pooling, void *stream, lscomp_plan **plan)
+{
+    return plan_create_t<uint16_t>(ws, stacks, n, bins, pooling, stream, reinterpret_cast<PlanImpl **>(plan));
+}
+
+int lscomp_plan_create_u32(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, const uint32_t bins[4],
+                           float pooling, void *stream, lscomp_plan **plan)
+{
+    return plan_create_t<uint32_t>(ws, stacks, n, bins, pooling, stream, reinterpret_cast<PlanImpl **>(plan));
+}
+
+int lscomp_plan_run(lscomp_plan *plan, void *stream, uint64_t *stream_len, uint64_t *ref_size)
+{
+    return plan_run(reinterpret_cast<PlanImpl *>(plan), stream, stream_len, ref_size);
+}
+
+int lscomp_plan_destroy(lscomp_plan *plan)
+{
+    plan_free(reinterpret_cast<PlanImpl *>(plan));
+    return LSCOMP_OK;
 }
 
 }  // extern "C"

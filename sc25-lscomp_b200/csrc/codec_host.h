@@ -6,6 +6,8 @@
 #include <stdint.h>
 #include <atomic>
 #include <mutex>
+#include <utility>
+#include <vector>
 #include "lscomp.h"
 #include "codec_kernels.cuh"
 
@@ -201,36 +203,52 @@ inline double unit_fill(const Geom &g, uint32_t wpg)
     return (double)units / (double)(wpg * ((units + wpg - 1) / wpg));
 }
 
-// Shape of the encoder CTA.  The lossless uint16 kernel is bound by its
-// producer and writer warps and keeps LSC_ENC_GROUPS x LSC_ENC_WPG; the lossy
-// one is bound by its compute warps, and when groups of 7 warps fill a
-// tile's unit slots clearly better than groups of 8 (a block-row of 195
-// blocks: 25 units, 89% against 78%) it runs with 7 (measured on B200:
-// CSSI-like lossy compress 2.71 -> 2.59 ms; XPCS-like tiles of 32 units keep 8).
+// Shape of the encoder CTA when no tuned choice is known (shape < 0): the
+// lossless uint16 kernel is bound by its producer and writer warps and keeps
+// LSC_ENC_GROUPS x LSC_ENC_WPG; the lossy one is bound by its compute warps,
+// and when groups of 7 warps fill a tile's unit slots clearly better than
+// groups of 8 (a block-row of 195 blocks: 25 units, 89% against 78%) it runs
+// with 7 (measured on B200: CSSI-like lossy compress 2.71 -> 2.59 ms;
+// XPCS-like tiles of 32 units keep 8).  shape 0 / 1 force 2 x 8 / 2 x 7
+// (uint16 only; uint32 always runs 2 x 8).
 template <typename T, int VEC, int BINS, bool POOL, bool BATCH>
-inline int launch_enc_t(const EncArgs<T> &a, int sm_count, cudaStream_t st)
+inline int launch_enc_t(const EncArgs<T> &a, int shape, int sm_count, cudaStream_t st)
 {
-    if constexpr (sizeof(T) == 2 && BINS != BINS_IDENT && !BATCH && LSC_ENC_GROUPS == 2 && LSC_ENC_WPG == 8) {
-        if (unit_fill(a.g, 7) > unit_fill(a.g, 8) + 0.05)
-            return launch_enc_w<T, VEC, BINS, POOL, 2, 7, BATCH>(a, sm_count, st);
+    if constexpr (sizeof(T) == 2 && LSC_ENC_GROUPS == 2 && LSC_ENC_WPG == 8) {
+        const bool seven = shape == 1 || (shape < 0 && BINS != BINS_IDENT && !BATCH &&
+                                          unit_fill(a.g, 7) > unit_fill(a.g, 8) + 0.05);
+        if (seven) return launch_enc_w<T, VEC, BINS, POOL, 2, 7, BATCH>(a, sm_count, st);
     }
     return launch_enc_w<T, VEC, BINS, POOL, LSC_ENC_GROUPS, LSC_ENC_WPG, BATCH>(a, sm_count, st);
 }
 
 template <typename T, int VEC, bool BATCH>
-inline int launch_enc_v(const EncArgs<T> &a, int layout, bool pool, int sm, cudaStream_t st)
+inline int launch_enc_v(const EncArgs<T> &a, int layout, bool pool, int shape, int sm, cudaStream_t st)
 {
     if (layout == BINS_IDENT)
-        return pool ? launch_enc_t<T, VEC, BINS_IDENT, true, BATCH>(a, sm, st)
-                    : launch_enc_t<T, VEC, BINS_IDENT, false, BATCH>(a, sm, st);
+        return pool ? launch_enc_t<T, VEC, BINS_IDENT, true, BATCH>(a, shape, sm, st)
+                    : launch_enc_t<T, VEC, BINS_IDENT, false, BATCH>(a, shape, sm, st);
     if (layout == BINS_EQUAL)
-        return pool ? launch_enc_t<T, VEC, BINS_EQUAL, true, BATCH>(a, sm, st)
-                    : launch_enc_t<T, VEC, BINS_EQUAL, false, BATCH>(a, sm, st);
+        return pool ? launch_enc_t<T, VEC, BINS_EQUAL, true, BATCH>(a, shape, sm, st)
+                    : launch_enc_t<T, VEC, BINS_EQUAL, false, BATCH>(a, shape, sm, st);
     if (layout == BINS_MONO)
-        return pool ? launch_enc_t<T, VEC, BINS_MONO, true, BATCH>(a, sm, st)
-                    : launch_enc_t<T, VEC, BINS_MONO, false, BATCH>(a, sm, st);
-    return pool ? launch_enc_t<T, VEC, BINS_GENERAL, true, BATCH>(a, sm, st)
-                : launch_enc_t<T, VEC, BINS_GENERAL, false, BATCH>(a, sm, st);
+        return pool ? launch_enc_t<T, VEC, BINS_MONO, true, BATCH>(a, shape, sm, st)
+                    : launch_enc_t<T, VEC, BINS_MONO, false, BATCH>(a, shape, sm, st);
+    return pool ? launch_enc_t<T, VEC, BINS_GENERAL, true, BATCH>(a, shape, sm, st)
+                : launch_enc_t<T, VEC, BINS_GENERAL, false, BATCH>(a, shape, sm, st);
+}
+
+// Encoder launch with the widest row access `vec` allows.
+template <typename T, bool BATCH>
+inline int launch_enc_any(const EncArgs<T> &a, int vec, int layout, bool pool, int shape, int sm, cudaStream_t st)
+{
+    switch (vec) {
+    case 16: return launch_enc_v<T, 16, BATCH>(a, layout, pool, shape, sm, st);
+    case 4: return launch_enc_v<T, 4, BATCH>(a, layout, pool, shape, sm, st);
+    default:
+        if constexpr (sizeof(T) == 2) return launch_enc_v<T, 2, BATCH>(a, layout, pool, shape, sm, st);
+        return LSCOMP_ERR_ARG;
+    }
 }
 
 template <typename T, int VEC>
@@ -258,6 +276,77 @@ inline int read_ctl(lscomp_workspace *ws, cudaStream_t st)
     e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return cuda_status(e);
     return dev_status(ws->h_ctl->error);
+}
+
+// ---------------------------------------------------------------- tuner
+// Launch configuration of one call: encoder CTA shape (-1: the rule of
+// launch_enc_t, 0: 2 x 8 warps, 1: 2 x 7) and the most blocks a tile holds.
+struct TuneCfg {
+    int shape;
+    uint32_t tile_blocks;
+};
+
+constexpr uint8_t kTuneCompress = 0, kTuneBatch = 1, kTuneDecompress = 2;
+
+// What a choice is kept for: element size, bins layout, pooling on/off,
+// call kind, row access width and blocks per block-row (0 for batches).
+struct TuneKey {
+    uint8_t es, layout, pool, kind, vec;
+    uint32_t bzb;
+};
+
+int tune_mode();  // 1: tune keys not in the table on first use
+bool tune_lookup(const TuneKey &k, TuneCfg &c);  // counts a hit when found
+void tune_store(const TuneKey &k, const TuneCfg &c, const std::vector<std::pair<TuneCfg, float>> &times);
+std::vector<TuneCfg> tune_candidates(int es, int kind);
+
+constexpr int kTuneReps = 3;
+// Single stacks of fewer tiles than this many per SM are not tuned (their
+// time is launch latency and the scan's tail; the rules serve them)
+constexpr int kTuneMinTilesPerSm = 4;
+
+// The configuration for `key`: the table's, else (tuning on, may_tune, stream
+// not being captured) the fastest candidate, each timed with CUDA events over
+// kTuneReps calls after one untimed call; else `rule`.  run(cfg) enqueues
+// one complete call on st (control block cleared, kernel launched) and
+// returns its launch status; the caller holds the workspace lock.  A
+// candidate whose launch or device status fails ends the tuning with
+// `rule` and nothing stored.
+template <class Run>
+inline TuneCfg tune_choose(lscomp_workspace *ws, const TuneKey &key, const TuneCfg &rule, bool may_tune,
+                           cudaStream_t st, Run run)
+{
+    TuneCfg c;
+    if (tune_lookup(key, c)) return c;
+    if (!may_tune || !tune_mode()) return rule;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return rule;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cudaEventCreate(&e0) != cudaSuccess) return rule;
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return rule;
+    }
+    std::vector<std::pair<TuneCfg, float>> times;
+    bool ok = true;
+    for (const TuneCfg &cand : tune_candidates(key.es, key.kind)) {
+        ok = run(cand) == LSCOMP_OK && read_ctl(ws, st) == LSCOMP_OK;
+        if (ok) ok = cudaEventRecord(e0, st) == cudaSuccess;
+        for (int i = 0; ok && i < kTuneReps; i++) ok = run(cand) == LSCOMP_OK;
+        if (ok) ok = cudaEventRecord(e1, st) == cudaSuccess && read_ctl(ws, st) == LSCOMP_OK;
+        float ms = 0.f;
+        if (ok) ok = cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess;
+        if (!ok) break;
+        times.push_back({cand, ms / kTuneReps});
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (!ok || times.empty()) return rule;
+    size_t best = 0;
+    for (size_t i = 1; i < times.size(); i++)
+        if (times[i].second < times[best].second) best = i;
+    tune_store(key, times[best].first, times);
+    return times[best].first;
 }
 
 }  // namespace lsc_host

@@ -386,16 +386,19 @@ __device__ __forceinline__ void quant(Row<uint32_t> &v, const Codec &c, uint32_t
 // of row a then the 4 of row b, as one Row
 __device__ __forceinline__ Row<uint16_t> pool_rows(const Row<uint16_t> &a, const Row<uint16_t> &b)
 {
+    // x = the first values of two pairs, y = the second ones, in 16-bit
+    // halves; floor((x + y) / 2) = (x & y) + ((x ^ y) >> 1) per half, which
+    // stays below 2^16 and carries nothing into the other half
     Row<uint16_t> p;
 #pragma unroll
     for (int i = 0; i < 2; i++) {
         const Row<uint16_t> &s = i ? b : a;
-        uint32_t m0 = ((s.w[0] & 0xffffu) + (s.w[0] >> 16)) >> 1;
-        uint32_t m1 = ((s.w[1] & 0xffffu) + (s.w[1] >> 16)) >> 1;
-        uint32_t m2 = ((s.w[2] & 0xffffu) + (s.w[2] >> 16)) >> 1;
-        uint32_t m3 = ((s.w[3] & 0xffffu) + (s.w[3] >> 16)) >> 1;
-        p.w[2 * i] = m0 | (m1 << 16);
-        p.w[2 * i + 1] = m2 | (m3 << 16);
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const uint32_t x = __byte_perm(s.w[2 * h], s.w[2 * h + 1], 0x5410u);
+            const uint32_t y = __byte_perm(s.w[2 * h], s.w[2 * h + 1], 0x7632u);
+            p.w[2 * i + h] = (x & y) + (((x ^ y) >> 1) & 0x7fff7fffu);
+        }
     }
     return p;
 }
@@ -456,17 +459,21 @@ __device__ __forceinline__ uint32_t min2u16(uint32_t a, uint32_t b)
     return d;
 }
 
-// (w - B) mod 2^16 in each 16-bit half (no borrow between the halves)
-__device__ __forceinline__ uint32_t sub16x2(uint32_t w, uint32_t B)
+// per 16-bit half: (w + NB) mod 2^16 (no carry between the halves); with NB
+// = (2^16 - b0) mod 2^16 in both halves this is (v - b0) mod 2^16
+__device__ __forceinline__ uint32_t add16x2(uint32_t w, uint32_t NB)
 {
-    return ((w | 0x80008000u) - (B & 0x7fff7fffu)) ^ ((w ^ ~B) & 0x80008000u);
+    uint32_t d;
+    asm("add.u16x2 %0, %1, %2;" : "=r"(d) : "r"(w), "r"(NB));
+    return d;
 }
 
-// per 16-bit half: min over the row of (v - b0) mod 2^16 (B = b0 in both halves)
-__device__ __forceinline__ uint32_t min16_from(const Row<uint16_t> &v, uint32_t B, uint32_t acc)
+// per 16-bit half: min over the row of (v - b0) mod 2^16 (NB = -b0 mod 2^16
+// in both halves)
+__device__ __forceinline__ uint32_t min16_from(const Row<uint16_t> &v, uint32_t NB, uint32_t acc)
 {
 #pragma unroll
-    for (int i = 0; i < 4; i++) acc = min2u16(acc, sub16x2(v.w[i], B));
+    for (int i = 0; i < 4; i++) acc = min2u16(acc, add16x2(v.w[i], NB));
     return acc;
 }
 
@@ -896,7 +903,8 @@ __device__ __forceinline__ uint32_t block_header(const Row<T> &A, const Row<T> &
             // comes from a value >= bin0 when there is one, since every wrapped
             // difference (v < bin0) is larger; bin0 > 65535 leaves none
             if (b0 <= 0xffffu) {
-                const uint32_t m = min16_from(B, b0 * 0x10001u, min16_from(A, b0 * 0x10001u, 0xffffffffu));
+                const uint32_t NB = ((0x10000u - b0) & 0xffffu) * 0x10001u;
+                const uint32_t m = min16_from(B, NB, min16_from(A, NB, 0xffffffffu));
                 mn = min(m & 0xffffu, m >> 16);
             } else {
                 mn = 0xffffu;

@@ -129,6 +129,16 @@ def load_library() -> ctypes.CDLL:
     for sfx in ("u16", "u32"):
         getattr(lib, f"lscomp_compress_batch_{sfx}").argtypes = [vp, ctypes.POINTER(LscompStack), u32, bins_t, f32,
                                                                  pu64, pu64, vp]
+        getattr(lib, f"lscomp_plan_create_{sfx}").argtypes = [vp, ctypes.POINTER(LscompStack), u32, bins_t, f32, vp,
+                                                              ctypes.POINTER(vp)]
+    lib.lscomp_plan_run.argtypes = [vp, vp, pu64, pu64]
+    lib.lscomp_plan_destroy.argtypes = [vp]
+    lib.lscomp_tune_mode.argtypes = [ctypes.c_int]
+    lib.lscomp_tune_hits.restype = u64
+    lib.lscomp_tune_report.restype = u64
+    lib.lscomp_tune_report.argtypes = [ctypes.c_char_p, u64]
+    lib.lscomp_tune_save.argtypes = [ctypes.c_char_p]
+    lib.lscomp_tune_load.argtypes = [ctypes.c_char_p]
     _lib = lib
     return lib
 
@@ -239,6 +249,103 @@ def compress_batch(ws: Workspace, items, bins, pooling: float, stream=None):
                                                       ctypes.c_void_p(_stream_handle(stream)))
     _check(st, f"lscomp_compress_batch_{sfx}")
     return [(int(sl[i]), int(rs[i])) for i in range(n)]
+
+
+class Plan:
+    """A compression captured once as a CUDA graph (lscomp_plan_*): the same
+    items as compress_batch (one item: the single-stack kernel), replayed by
+    run() on new contents of the same buffers.  Creating it runs one ordinary
+    call through ws (the streams are written)."""
+
+    def __init__(self, ws: Workspace, items, bins, pooling: float, stream=None):
+        lib = load_library()
+        self._lib = lib
+        self.handle = None
+        n = len(items)
+        if n == 0:
+            raise ValueError("a plan holds at least one stack")
+        sfx = _suffix(items[0][0])
+        arr = (LscompStack * n)()
+        for i, (d_in, dims, d_out) in enumerate(items):
+            if _suffix(d_in) != sfx:
+                raise ValueError("a plan holds one element type")
+            x, y, z = (int(v) for v in dims)
+            arr[i] = LscompStack(d_in.data_ptr(), x, y, z, d_out.data_ptr(), d_out.numel() * d_out.element_size())
+        self.n = n
+        self._keep = items  # the buffers must outlive the plan
+        h = ctypes.c_void_p()
+        _check(getattr(lib, f"lscomp_plan_create_{sfx}")(ws.handle, arr, n, _bins(bins), ctypes.c_float(pooling),
+                                                         ctypes.c_void_p(_stream_handle(stream)), ctypes.byref(h)),
+               f"lscomp_plan_create_{sfx}")
+        self.handle = h
+
+    def run(self, stream=None):
+        """Replay; returns [(stream_len, ref_size), ...]."""
+        sl = (ctypes.c_uint64 * self.n)()
+        rs = (ctypes.c_uint64 * self.n)()
+        _check(self._lib.lscomp_plan_run(self.handle, ctypes.c_void_p(_stream_handle(stream)), sl, rs),
+               "lscomp_plan_run")
+        return [(int(sl[i]), int(rs[i])) for i in range(self.n)]
+
+    def close(self):
+        if self.handle:
+            self._lib.lscomp_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def tune_mode(mode: Optional[int] = None) -> int:
+    """Launch-configuration tuning: 1 on (tune keys on first use), 0 off;
+    None only queries.  Returns the previous mode."""
+    return int(load_library().lscomp_tune_mode(-1 if mode is None else int(mode)))
+
+
+def tune_hits() -> int:
+    """Calls so far that used a configuration from the tuner's table."""
+    return int(load_library().lscomp_tune_hits())
+
+
+def tune_clear() -> None:
+    _check(load_library().lscomp_tune_clear(), "lscomp_tune_clear")
+
+
+def tune_report() -> str:
+    """The tuner's table as text (see lscomp_tune_report in include/lscomp.h)."""
+    lib = load_library()
+    n = int(lib.lscomp_tune_report(None, 0))
+    buf = ctypes.create_string_buffer(n)
+    lib.lscomp_tune_report(buf, n)
+    return buf.value.decode()
+
+
+def tune_table() -> list:
+    """The tuner's table parsed: one dict per key."""
+    out = []
+    for line in tune_report().splitlines():
+        head, *cands = line.split(" | ")
+        key, cfg = head.split(" -> ")
+        es, layout, pool, kind, vec, bzb = (int(v) for v in key.split())
+        shape, tb = (int(v) for v in cfg.split())
+        times = []
+        for c in cands:
+            cs, ct, ms = c.split()
+            times.append({"shape": int(cs), "tile_blocks": int(ct), "ms": float(ms)})
+        out.append({"es": es, "layout": layout, "pool": pool, "kind": ("compress", "batch", "decompress")[kind],
+                    "vec": vec, "bzb": bzb, "shape": shape, "tile_blocks": tb, "times": times})
+    return out
+
+
+def tune_save(path: str) -> None:
+    _check(load_library().lscomp_tune_save(os.fsencode(path)), "lscomp_tune_save")
+
+
+def tune_load(path: str) -> None:
+    _check(load_library().lscomp_tune_load(os.fsencode(path)), "lscomp_tune_load")
 
 
 def container_header(elem_bytes: int, dims, bins, pooling: float, stream_len: int, ref_size: int) -> bytes:
