@@ -39,8 +39,6 @@
 //   LSC_WRITERS       writer warps per encoder CTA (1 or 2)
 //   LSC_LOOKBACK      0: 32-wide look-back to the nearest inclusive prefix,
 //                     1: 256-wide look-back bounded by the writer's previous tile
-//   LSC_DEC_HOIST     1: the decoder issues all payload loads of a warp's
-//                     units before transposing any of them
 //   LSC_DEC_CTAS      decoder CTAs per SM the register budget is sized for
 //   LSC_ENC_GROUPS    compute groups per encoder CTA (tiles in flight)
 //   LSC_ENC_WPG       warps per compute group
@@ -49,9 +47,6 @@
 #endif
 #ifndef LSC_LOOKBACK
 #define LSC_LOOKBACK 0
-#endif
-#ifndef LSC_DEC_HOIST
-#define LSC_DEC_HOIST 0
 #endif
 #ifndef LSC_DEC_CTAS
 #define LSC_DEC_CTAS 6  // decoder CTAs per SM the register budget is sized for (shared memory allows 6)
@@ -542,14 +537,19 @@ __device__ __forceinline__ void row_values(uint32_t P[][2], Row<uint32_t> &v, ui
     }
 }
 
+// both 16-bit halves times bin, each product kept mod 2^16 as the
+// reference's uint16 store keeps it: the low half of w * bin is the first
+// product, the high half of (w & 0xffff0000) * bin the second
+__device__ __forceinline__ uint32_t mul16x2(uint32_t w, uint32_t bin)
+{
+    return __byte_perm(w * bin, (w & 0xffff0000u) * bin, 0x7610u);
+}
+
 __device__ __forceinline__ void dequant(Row<uint16_t> &v, uint32_t bin)
 {
     if (bin == 1u) return;
 #pragma unroll
-    for (int i = 0; i < 4; i++) {
-        uint32_t lo = (v.w[i] & 0xffffu) * bin, hi = (v.w[i] >> 16) * bin;
-        v.w[i] = (lo & 0xffffu) | (hi << 16);
-    }
+    for (int i = 0; i < 4; i++) v.w[i] = mul16x2(v.w[i], bin);
 }
 
 __device__ __forceinline__ void dequant(Row<uint32_t> &v, uint32_t bin)
@@ -563,12 +563,11 @@ __device__ __forceinline__ void dequant(Row<uint32_t> &v, uint32_t bin)
 __device__ __forceinline__ Row<uint16_t> unpool_row(const Row<uint16_t> &q, bool second, uint32_t bin)
 {
     Row<uint16_t> v;
-    const uint32_t a = q.w[second ? 2 : 0], b = q.w[second ? 3 : 1];
-    uint32_t x0 = (a & 0xffffu) * bin, x1 = (a >> 16) * bin, x2 = (b & 0xffffu) * bin, x3 = (b >> 16) * bin;
-    v.w[0] = (x0 & 0xffffu) | (x0 << 16);
-    v.w[1] = (x1 & 0xffffu) | (x1 << 16);
-    v.w[2] = (x2 & 0xffffu) | (x2 << 16);
-    v.w[3] = (x3 & 0xffffu) | (x3 << 16);
+    const uint32_t a = mul16x2(q.w[second ? 2 : 0], bin), b = mul16x2(q.w[second ? 3 : 1], bin);
+    v.w[0] = __byte_perm(a, 0u, 0x1010u);  // first value in both halves
+    v.w[1] = __byte_perm(a, 0u, 0x3232u);  // second value in both halves
+    v.w[2] = __byte_perm(b, 0u, 0x1010u);
+    v.w[3] = __byte_perm(b, 0u, 0x3232u);
     return v;
 }
 
@@ -669,14 +668,13 @@ constexpr uint32_t kMaxTilePayload = 32768;
 
 struct DecSmem {
     alignas(16) uint8_t pay[kMaxTilePayload + 32];  // the tile's payload (TMA destination)
-    uint64_t pay_full;                               // its landing
+    uint32_t off[kMaxTileBlocks];                    // offset of each block inside its warp's 32 blocks
+    uint8_t hdr[kMaxTileBlocks];                     // header byte of each block
+    uint32_t wsum[kWarps];                           // payload bytes of each warp's 32 blocks
     uint32_t br_rel[kMaxTileBlocks];
     uint8_t br_rows[kMaxTileBlocks];
-    uint8_t hdr[kMaxTileBlocks];
-    uint32_t off[kMaxTileBlocks];
-    unsigned long long base;
+    uint64_t pay_full;                               // the payload's landing
     uint32_t pay_mis;                                // byte offset of the payload's first byte in pay
-    uint32_t flag_ok;
 };
 
 // ---------------------------------------------------------------- scan
@@ -1484,32 +1482,37 @@ __device__ __forceinline__ void dec_unit(const DecArgs<T> &a, const TileInfo &ti
 // One CTA per tile: header bytes -> in-tile offsets -> plane words of each
 // block -> values scattered to the output rows
 // (lsCOMP/src/cuLSZ_kernel.cu:1440-1640).  Every element of the tile is
-// written, zeros for blocks of rate 0.
+// written, zeros for blocks of rate 0.  The in-tile offsets take one
+// barrier: thread b scans block b's size inside its warp, the warps' totals
+// meet in shared memory, and each block's offset is its in-warp offset plus
+// the totals of the warps before it (kept one per lane, read by shuffle).
+// Thread 0's bulk copy of the payload is in flight meanwhile.
 template <typename T, int VEC>
 __global__ void __launch_bounds__(kThreads, LSC_DEC_CTAS) dec_kernel(const DecArgs<T> a)
 {
     constexpr int NG = Elem<T>::kGroups;
+    static_assert(kThreads >= kMaxTileBlocks && kWarps <= 32, "one thread per block of a tile");
     __shared__ DecSmem sm;
     const Geom &g = a.g;
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t jb = lane & 7, r = lane >> 3;
     const unsigned long long t = blockIdx.x;
     if (t >= g.ntiles) return;
+    const unsigned long long base = a.tile_off[t], end = a.tile_off[t + 1];
 
-    // thread 0: the tile's payload [R + tile_off[t], R + tile_off[t+1]) into
-    // shared memory with one bulk copy, overlapping the header scan; the
-    // range is clamped to the readable stream and to one tile's maximum
+    // thread 0: the tile's payload [R + base, R + end) into shared memory
+    // with one bulk copy; the range is clamped to the readable stream and to
+    // one tile's maximum
     if (tid == 0) {
         mbar_init(&sm.pay_full, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        const unsigned long long b0 = a.tile_off[t], b1 = a.tile_off[t + 1];
         uint32_t tx = 0;
         sm.pay_mis = 0;
-        if (b1 >= b0 && b1 - b0 <= kMaxTilePayload && g.R + b1 <= a.cap) {
-            const uintptr_t base = reinterpret_cast<uintptr_t>(a.in);
-            const uintptr_t A0 = (base + 15) & ~(uintptr_t)15;
-            const uintptr_t A1 = (base + a.cap) & ~(uintptr_t)15;
-            const uintptr_t ga = base + g.R + b0, ge = base + g.R + b1;
+        if (end >= base && end - base <= kMaxTilePayload && g.R + end <= a.cap) {
+            const uintptr_t bp = reinterpret_cast<uintptr_t>(a.in);
+            const uintptr_t A0 = (bp + 15) & ~(uintptr_t)15;
+            const uintptr_t A1 = (bp + a.cap) & ~(uintptr_t)15;
+            const uintptr_t ga = bp + g.R + base, ge = bp + g.R + end;
             const uintptr_t gs = ga & ~(uintptr_t)15;
             uintptr_t cs = gs > A0 ? gs : A0;
             uintptr_t ce = (ge + 15) & ~(uintptr_t)15;
@@ -1532,70 +1535,65 @@ __global__ void __launch_bounds__(kThreads, LSC_DEC_CTAS) dec_kernel(const DecAr
     if (!g.chunked) {
         if (tid < ti.nbr) {
             uint32_t nrows;
-            unsigned long long rs = brow_start(g, ti.rho0 + tid, nrows);
+            const unsigned long long rs = brow_start(g, ti.rho0 + tid, nrows);
             sm.br_rel[tid] = (uint32_t)((rs - row0) * g.Z);
             sm.br_rows[tid] = (uint8_t)nrows;
         }
     } else if (tid == 0) {
         sm.br_rows[0] = (uint8_t)n0;
     }
-    for (uint32_t b = tid; b < ti.nblk; b += kThreads) sm.hdr[b] = a.in[ti.k0 + b];
-    __syncthreads();
-    if (warp == 0) {
-        const uint32_t agg = tile_scan(sm.hdr, sm.off, ti.nblk);
-        if (lane == 0) {
-            const unsigned long long base = a.tile_off[t];
-            sm.base = base;
-            sm.flag_ok = 1u;
-            if (g.R + base + agg > a.cap) {
-                raise_error(a.ctl, DEV_ERR_CAPACITY);
-                sm.flag_ok = 0;
-            } else if (a.tile_off[t + 1] != base + agg) {
-                raise_error(a.ctl, DEV_ERR_CORRUPT);
-                sm.flag_ok = 0;
-            }
+    {
+        // block tid: header byte, size, offset inside the warp's 32 blocks
+        const uint32_t h = tid < ti.nblk ? a.in[ti.k0 + tid] : 0u;
+        const uint32_t sz = (h & 0x1fu) << (3u - (h >> 7));  // rate planes of 8 bytes, or 4 when pooled
+        uint32_t inc = sz;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t x = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= (uint32_t)o) inc += x;
         }
+        sm.hdr[tid] = (uint8_t)h;
+        sm.off[tid] = inc - sz;
+        if (lane == 31) sm.wsum[warp] = inc;
     }
     __syncthreads();
+    // lane w < kWarps: bytes before warp w's blocks; agg: the whole tile
+    uint32_t wpre;
+    {
+        const uint32_t v = lane < (uint32_t)kWarps ? sm.wsum[lane] : 0u;
+        uint32_t inc = v;
+#pragma unroll
+        for (int o = 1; o < kWarps; o <<= 1) {
+            const uint32_t x = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= (uint32_t)o) inc += x;
+        }
+        wpre = inc - v;
+    }
+    const uint32_t agg = __shfl_sync(0xffffffffu, wpre, kWarps - 1) + sm.wsum[kWarps - 1];
+    bool ok = true;
+    if (g.R + base + agg > a.cap) {
+        ok = false;
+        if (tid == 0) raise_error(a.ctl, DEV_ERR_CAPACITY);
+    } else if (end != base + agg) {
+        ok = false;
+        if (tid == 0) raise_error(a.ctl, DEV_ERR_CORRUPT);
+    }
     // the payload copy must land before the CTA returns or reads it
     const bool landed = mbar_wait_landed(&sm.pay_full, 0);
-    if (!sm.flag_ok || !__syncthreads_and(landed)) return;
+    if (!ok || !__all_sync(0xffffffffu, landed)) return;
 
     const uint8_t *const pay = sm.pay + sm.pay_mis;
     const unsigned long long ebase = row0 * g.Z;  // element index of the tile's first row
     const uint32_t nunits = (ti.nblk + 7) >> 3;
-#if LSC_DEC_HOIST
-    // all plane words of the warp's units first, so their loads overlap
-    constexpr int UMAX = Elem<T>::kTileBlocks / 8 / kWarps;  // units per warp per tile
-    uint32_t Y[UMAX][NG][4];
-    uint32_t hq[UMAX];
-#pragma unroll
-    for (int q = 0; q < UMAX; q++) {
-        const uint32_t u = warp + (uint32_t)q * kWarps;
-        hq[q] = 0;
-        if (u < nunits) {
-            const uint32_t b = u * 8 + jb;
-            const bool active = b < ti.nblk;
-            hq[q] = active ? sm.hdr[b] : 0u;
-            dec_load<T>(pay + (active ? sm.off[b] : 0u), hq[q], r, Y[q]);
-        }
-    }
-#pragma unroll
-    for (int q = 0; q < UMAX; q++) {
-        const uint32_t u = warp + (uint32_t)q * kWarps;
-        if (u < nunits)
-            dec_unit<T, VEC>(a, ti, sm, Y[q], hq[q], u * 8 + jb, r, ebase);
-    }
-#else
     for (uint32_t u = warp; u < nunits; u += kWarps) {
         const uint32_t b = u * 8 + jb;
         const bool active = b < ti.nblk;
         const uint32_t h = active ? sm.hdr[b] : 0u;
+        const uint32_t o = sm.off[active ? b : 0] + __shfl_sync(0xffffffffu, wpre, u >> 2);  // 4 units per warp's 32 blocks
         uint32_t Y[NG][4];
-        dec_load<T>(pay + (active ? sm.off[b] : 0u), h, r, Y);
+        dec_load<T>(pay + (active ? o : 0u), h, r, Y);
         dec_unit<T, VEC>(a, ti, sm, Y, h, b, r, ebase);
     }
-#endif
 }
 
 }  // namespace lsc
