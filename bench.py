@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--serve", type=float, default=0.0,
                     help="serving benchmark: Poisson arrivals at this many requests per second (its own JSON line)")
     ap.add_argument("--serve-seconds", type=float, default=10.0)
+    ap.add_argument("--batch-frames", type=int, default=16, help="largest frame count of a batch stack")
     ap.add_argument("--batch", type=int, default=0,
                     help="batched-stacks benchmark over this many stacks (its own JSON line)")
     return ap.parse_args()
@@ -240,51 +241,73 @@ def barrier(world):
         dist.barrier()
 
 
-def batch_workload(n, seed=11):
-    """Seeded batch of detector stacks: frames U{1..16}, frame height and
-    width U{100..1024} (non-multiples of 8 included), half CSSI-like and half
-    XPCS-like."""
-    import lscomp
+BATCH_SETTINGS = [((1, 1, 1, 1), 1.0), ((3, 5, 10, 15), None), ((5, 10, 15, 20), None)]
+BATCH_P = (0.3, 0.5, 0.8)
 
+
+def batch_workload(n, max_frames, seed=11):
+    """Seeded batch description: per stack dims (frames U{1..max_frames},
+    frame height and width U{100..2048}, non-multiples of 8 included), data
+    kind (CSSI-like or XPCS-like, alternating) and settings (bins from
+    {lossless, 3 5 10 15, 5 10 15 20}; lossy stacks take p from
+    {0.3, 0.5, 0.8}, lossless stacks p = 1)."""
     rng = np.random.default_rng(seed)
-    stacks = []
+    out = []
     for i in range(n):
-        dims = (int(rng.integers(1, 17)), int(rng.integers(100, 1025)), int(rng.integers(100, 1025)))
+        dims = (int(rng.integers(1, max_frames + 1)), int(rng.integers(100, 2049)), int(rng.integers(100, 2049)))
         kind = "cssi" if i % 2 == 0 else "xpcs"
-        stacks.append((dims, getattr(lscomp, f"synth_{kind}")(dims, seed=seed + i)))
-    return stacks
+        bins, p = BATCH_SETTINGS[int(rng.integers(0, len(BATCH_SETTINGS)))]
+        if p is None:
+            p = BATCH_P[int(rng.integers(0, len(BATCH_P)))]
+        out.append({"dims": dims, "kind": kind, "bins": bins, "p": p, "seed": seed + i})
+    return out
 
 
 def bench_batch(args, local):
-    """Batched compress: one lscomp_compress_batch_u16 call over all stacks
-    against one call per stack (asynchronous, and synchronous with the size
-    read back as the reference's host API does).  Inputs resident in HBM."""
+    """Batched compress of many uneven stacks, each with its own bins and
+    pooling threshold: one lscomp_compress_batch_ex_u16 call, and the same
+    captured once as a CUDA graph (lscomp_plan_*), against one plain call
+    per stack and one plain call per frame (and, for --impl reference, the
+    reference's host API called per stack).  Inputs resident in HBM; each
+    stack is generated on the host and copied to its slice of one device
+    buffer, so host memory holds one stack at a time."""
     import torch
 
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream()
-    stacks = batch_workload(args.batch)
-    frames = sum(d[0] for d, _ in stacks)
-    nbytes = sum(h.size * 2 for _, h in stacks)
-    # one input and one output buffer, each stack at a 16-byte boundary
+    desc = batch_workload(args.batch, args.batch_frames)
+    frames = sum(d["dims"][0] for d in desc)
+    nel = [d["dims"][0] * d["dims"][1] * d["dims"][2] for d in desc]
+    nbytes = 2 * sum(nel)
+
+    def cap_of(dims):
+        nb = dims[0] * ((dims[1] + 7) // 8) * ((dims[2] + 7) // 8)
+        return (nb + 3) // 4 * 4 + 128 * nb
+
     offs_in, offs_out, n_in, n_out = [], [], 0, 0
-    for dims, h in stacks:
+    for d, n in zip(desc, nel):
         offs_in.append(n_in)
-        n_in += (h.size + 7) // 8 * 8
-        nb = dims[0] * ((dims[1] + 7) // 8) * ((dims[2] + 7) // 8)
+        n_in += (n + 7) // 8 * 8  # each stack at a 16-byte boundary
         offs_out.append(n_out)
-        n_out += ((nb + 3) // 4 * 4 + 128 * nb + 15) // 16 * 16
-    d_in_all = torch.zeros(n_in, dtype=torch.int16, device=dev)
+        n_out += (cap_of(d["dims"]) + 15) // 16 * 16
+    d_in_all = torch.empty(n_in, dtype=torch.int16, device=dev)
     d_out_all = torch.zeros(n_out, dtype=torch.uint8, device=dev)
+    import lscomp
+
     items = []
-    for (dims, h), oi, oo in zip(stacks, offs_in, offs_out):
-        d = d_in_all[oi:oi + h.size]
-        d.copy_(torch.from_numpy(h.view(np.int16)))
-        nb = dims[0] * ((dims[1] + 7) // 8) * ((dims[2] + 7) // 8)
-        items.append((d, dims, d_out_all[oo:oo + (nb + 3) // 4 * 4 + 128 * nb]))
-    config = {"workload": f"{len(stacks)} stacks, frames U{{1..16}}, frame U{{100..1024}}^2 uint16, half CSSI-like "
-                          f"half XPCS-like", "frames": frames, "input_bytes": nbytes,
-              "modes": "lossless -b 1 1 1 1 -p 1; lossy -b 3 5 10 15 -p 0.5"}
+    for d, n, oi, oo in zip(desc, nel, offs_in, offs_out):
+        h = getattr(lscomp, f"synth_{d['kind']}")(d["dims"], seed=d["seed"])
+        d_in = d_in_all[oi:oi + n]
+        d_in.copy_(torch.from_numpy(h.view(np.int16).ravel()))
+        items.append((d_in, d["dims"], d_out_all[oo:oo + cap_of(d["dims"])], d["bins"], d["p"]))
+    del h
+    torch.cuda.synchronize()
+    config = {"workload": f"{len(desc)} stacks, frames U{{1..{args.batch_frames}}}, frame height and width "
+                          f"U{{100..2048}} uint16, CSSI-like and XPCS-like alternating; per stack bins from "
+                          f"{{lossless, 3 5 10 15, 5 10 15 20}} and p from {{0.3, 0.5, 0.8}} (lossless: p 1)",
+              "frames": frames, "input_bytes": nbytes,
+              "scaled_from": "2000 stacks with frames U{1..64} (about 150 GB of input, more than one GPU holds "
+                             "with worst-case stream buffers); frames per stack reduced"}
 
     def timed(fn, reps):
         for _ in range(max(args.warmup, 3)):
@@ -300,60 +323,69 @@ def bench_batch(args, local):
             ts.append(e0.elapsed_time(e1))
         return float(np.median(ts))
 
-    res = {}
+    def fps(ms):
+        return round(frames / ms * 1e3, 1)
+
     if args.impl == "reference":
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         from oracle import RefLib
 
         ref = RefLib()
-        for name, bins, p in MODES:
-            def loop_ref():
-                for d_in, dims, d_out in items:
-                    ref.compress(d_in.data_ptr(), d_out.data_ptr(), dims, bins, p, stream=stream.cuda_stream)
-            ms = timed(loop_ref, args.steps)
-            res[name] = {"per_stack_calls_ms": round(ms, 3), "frames_per_s": round(frames / ms * 1e3, 1)}
-        value = res["lossless"]["frames_per_s"]
+
+        def loop_ref():
+            for d_in, dims, d_out, bins, p in items:
+                ref.compress(d_in.data_ptr(), d_out.data_ptr(), dims, bins, p, stream=stream.cuda_stream)
+
+        ms = timed(loop_ref, args.steps)
         print(json.dumps({"metric": "batched compress frames per second (reference host API, one call per stack)",
-                          "value": value, "unit": "frames/s", "impl": "reference", "higher_is_better": True,
-                          "per_mode": res, "config": config}))
+                          "value": fps(ms), "unit": "frames/s", "impl": "reference", "higher_is_better": True,
+                          "per_stack_calls_ms": round(ms, 3), "config": config}))
         return
-    import lscomp
 
     ws = lscomp.Workspace(local)
-    for name, bins, p in MODES:
-        got = lscomp.compress_batch(ws, items, bins, p)
-        for (d_in, dims, d_out), (sl, rs) in zip(items[:: max(1, len(items) // 16)], got[:: max(1, len(items) // 16)]):
-            chk = torch.zeros(d_out.numel(), dtype=torch.uint8, device=dev)
-            assert lscomp.compress_into(ws, d_in, dims, bins, p, chk) == (sl, rs)
-            assert torch.equal(chk[:sl], d_out[:sl]), "batch stream differs from the single-stack stream"
-        t_batch = timed(lambda: lscomp.compress_batch(ws, items, bins, p), args.steps)
-        plan = lscomp.Plan(ws, items, bins, p)
-        assert plan.run() == got, "graph plan sizes differ from the batch call"
-        t_plan = timed(plan.run, args.steps)
-        plan.close()
+    got = lscomp.compress_batch_mixed(ws, items)
+    step = max(1, len(items) // 24)
+    for it, (sl, rs) in zip(items[::step], got[::step]):
+        d_in, dims, d_out, bins, p = it
+        chk = torch.zeros(d_out.numel(), dtype=torch.uint8, device=dev)
+        assert lscomp.compress_into(ws, d_in, dims, bins, p, chk) == (sl, rs)
+        assert torch.equal(chk[:sl], d_out[:sl]), "batch stream differs from the single-stack stream"
+    t_batch = timed(lambda: lscomp.compress_batch_mixed(ws, items), args.steps)
+    plan = lscomp.Plan(ws, items)
+    assert plan.run() == got, "graph plan sizes differ from the batch call"
+    t_plan = timed(plan.run, args.steps)
+    plan.close()
 
-        def loop_async():
-            for d_in, dims, d_out in items:
-                lscomp.compress_async(ws, d_in, dims, bins, p, d_out)
+    def loop_stack():
+        for d_in, dims, d_out, bins, p in items:
+            lscomp.compress_into(ws, d_in, dims, bins, p, d_out)
 
-        def loop_sync():
-            for d_in, dims, d_out in items:
-                lscomp.compress_into(ws, d_in, dims, bins, p, d_out)
+    t_stack = timed(loop_stack, args.steps)
+    # one plain call per frame, each frame a stack of its own; every frame
+    # writes the same scratch stream buffer (only the time is kept)
+    scratch = torch.empty(max(lscomp.max_stream_bytes((1, d["dims"][1], d["dims"][2])) for d in desc),
+                          dtype=torch.uint8, device=dev)
 
-        t_async = timed(loop_async, args.steps)
-        t_sync = timed(loop_sync, args.steps)
-        res[name] = {"batch_ms": round(t_batch, 3), "graph_plan_ms": round(t_plan, 3),
-                     "graph_plan_frames_per_s": round(frames / t_plan * 1e3, 1),
-                     "per_stack_async_ms": round(t_async, 3),
-                     "per_stack_sync_ms": round(t_sync, 3), "frames_per_s": round(frames / t_batch * 1e3, 1),
-                     "input_gbs": round(nbytes / t_batch / 1e6, 1),
-                     "speedup_vs_per_stack_async": round(t_async / t_batch, 2),
-                     "speedup_vs_per_stack_sync": round(t_sync / t_batch, 2)}
-    print(json.dumps({"metric": "batched compress frames per second (one lscomp_compress_batch_u16 call)",
-                      "value": res["lossless"]["frames_per_s"], "unit": "frames/s", "higher_is_better": True,
-                      "per_mode": res, "config": config, "tuned": tuned_summary(lscomp, ("batch",)),
-                      "timing": "CUDA events around each call, median of "
-                      f"{args.steps}; sizes read back to the host inside the batch call and the graph replay"}))
+    def loop_frame():
+        for d_in, dims, d_out, bins, p in items:
+            fsz = dims[1] * dims[2]
+            for f in range(dims[0]):
+                lscomp.compress_into(ws, d_in[f * fsz:(f + 1) * fsz], (1, dims[1], dims[2]), bins, p, scratch)
+
+    t_frame = timed(loop_frame, max(1, args.steps // 2))
+    res = {"batch_call_ms": round(t_batch, 3), "graph_plan_ms": round(t_plan, 3),
+           "per_stack_calls_ms": round(t_stack, 3), "per_frame_calls_ms": round(t_frame, 3),
+           "frames_per_s": {"graph_plan": fps(t_plan), "batch_call": fps(t_batch), "per_stack_calls": fps(t_stack),
+                            "per_frame_calls": fps(t_frame)},
+           "input_gbs_graph_plan": round(nbytes / t_plan / 1e6, 1),
+           "speedup_graph_plan_vs_per_frame": round(t_frame / t_plan, 2),
+           "speedup_graph_plan_vs_per_stack": round(t_stack / t_plan, 2)}
+    print(json.dumps({"metric": "batched compress frames per second (one graph replay of the mixed-settings "
+                                "batch launch)",
+                      "value": fps(t_plan), "unit": "frames/s", "higher_is_better": True, "results": res,
+                      "config": config, "tuned": tuned_summary(lscomp, ("batch",)),
+                      "timing": f"CUDA events around each call, median of {args.steps}; sizes read back to the "
+                                "host inside every batch call, graph replay and plain call"}))
 
 
 def tuned_summary(lscomp, kinds=("compress", "batch", "decompress")):

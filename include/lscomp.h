@@ -153,6 +153,18 @@ int lscomp_compress_batch_u32(lscomp_workspace *ws, const lscomp_stack *stacks, 
                               const uint32_t bins[4], float pooling, uint64_t *stream_len,
                               uint64_t *ref_size, void *stream);
 
+/* Batch compression with bins and pooling threshold per stack: bins[4 i ..
+   4 i + 3] and pooling[i] belong to stacks[i].  One launch still serves
+   all stacks (instantiated for a bins class that covers every stack's:
+   lossless and equal bins are special cases of increasing bins); each
+   stream equals the single-stack stream with that stack's settings. */
+int lscomp_compress_batch_ex_u16(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n,
+                                 const uint32_t *bins, const float *pooling, uint64_t *stream_len,
+                                 uint64_t *ref_size, void *stream);
+int lscomp_compress_batch_ex_u32(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n,
+                                 const uint32_t *bins, const float *pooling, uint64_t *stream_len,
+                                 uint64_t *ref_size, void *stream);
+
 /* Graph plans (no counterpart in the reference).  A plan fixes one
    compression -- n stacks (n = 1: the single-stack kernel, n > 1: the batch
    kernel), their buffers and shapes, bins and pooling threshold -- and
@@ -173,6 +185,11 @@ int lscomp_plan_create_u16(lscomp_workspace *ws, const lscomp_stack *stacks, uin
                            float pooling, void *stream, lscomp_plan **plan);
 int lscomp_plan_create_u32(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, const uint32_t bins[4],
                            float pooling, void *stream, lscomp_plan **plan);
+/* ... with bins and pooling threshold per stack, as lscomp_compress_batch_ex_* */
+int lscomp_plan_create_ex_u16(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, const uint32_t *bins,
+                              const float *pooling, void *stream, lscomp_plan **plan);
+int lscomp_plan_create_ex_u32(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, const uint32_t *bins,
+                              const float *pooling, void *stream, lscomp_plan **plan);
 int lscomp_plan_run(lscomp_plan *plan, void *stream, uint64_t *stream_len, uint64_t *ref_size);
 int lscomp_plan_destroy(lscomp_plan *plan);
 

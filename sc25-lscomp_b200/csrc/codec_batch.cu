@@ -80,15 +80,48 @@ inline bool batch_geoms(const lscomp_stack *stacks, uint32_t n, uint32_t tile_bl
     return true;
 }
 
+// Per-stack codecs (per_stack: bins[4 s .. 4 s + 3] and pooling[s] for stack
+// s; else bins[0..3] and pooling[0] for all) and the bins layout and pooling
+// flag one launch must be instantiated for to serve all of them: a common
+// layout if there is one, else the increasing-bins kernel when every stack's
+// bins increase (lossless and equal bins are special cases of it), else the
+// general one.
+inline bool batch_codecs(const uint32_t *bins, const float *pooling, bool per_stack, uint32_t n, bool wide,
+                         std::vector<Codec> &codec, int &layout, bool &pool)
+{
+    if (!bins || !pooling) return false;
+    codec.resize(n);
+    layout = -1;
+    bool mono = true;
+    pool = false;
+    for (uint32_t s = 0; s < n; s++) {
+        int l = 0;
+        if (per_stack || s == 0) {
+            if (!make_codec(bins + (per_stack ? 4ull * s : 0), pooling[per_stack ? s : 0], wide, codec[s], l)) return false;
+        } else {
+            codec[s] = codec[0];
+            l = layout;
+        }
+        if (s == 0) layout = l;
+        else if (l != layout) layout = -2;  // mixed
+        if (l == BINS_GENERAL) mono = false;
+        if (codec[s].pool_min <= 64) pool = true;
+    }
+    if (layout == -2) layout = mono ? BINS_MONO : BINS_GENERAL;
+    return true;
+}
+
 template <typename T>
-int compress_batch_t(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, const uint32_t bins[4],
-                     float pooling, uint64_t *stream_len, uint64_t *ref_size, void *stream)
+int compress_batch_t(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, const uint32_t *bins,
+                     const float *pooling, bool per_stack, uint64_t *stream_len, uint64_t *ref_size, void *stream)
 {
     if (!ws || (n && !stacks)) return LSCOMP_ERR_ARG;
     if (n == 0) return LSCOMP_OK;
-    Codec c;
+    std::vector<Codec> codec;
     int layout = 0;
-    if (!make_codec(bins, pooling, sizeof(T) == 4, c, layout)) return LSCOMP_ERR_ARG;
+    bool pool = false;
+    if (!batch_codecs(bins, pooling, per_stack, n, sizeof(T) == 4, codec, layout, pool)) return LSCOMP_ERR_ARG;
+    const Codec &c = codec[0];
     // every stack checked as lscomp_compress_* checks it; the narrowest
     // row access any stack allows is used for all
     std::vector<Geom> geom;
@@ -112,7 +145,6 @@ int compress_batch_t(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t 
     int prev = 0;
     cudaGetDevice(&prev);
     if (prev != ws->device) cudaSetDevice(ws->device);
-    const bool pool = c.pool_min <= 64;
     // one complete call with configuration cfg.  The descriptors are rebuilt
     // only when the tile size changes; the tuner synchronises the stream
     // before it changes configuration, so no pending copy reads the pinned
@@ -127,6 +159,7 @@ int compress_batch_t(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t 
             for (uint32_t s = 0; s < n; s++) {
                 BatchStack &b = ws->h_stacks[s];
                 b.g = geom[s];
+                b.c = codec[s];
                 b.in = stacks[s].d_in;
                 b.out = stacks[s].d_out;
                 b.cap = stacks[s].cap;
@@ -237,22 +270,23 @@ void plan_free(PlanImpl *p)
 constexpr uint32_t kPlanEpoch = 1;  // the graph clears the look-back words before every replay
 
 template <typename T>
-int plan_create_t(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, const uint32_t bins[4],
-                  float pooling, void *stream, PlanImpl **out)
+int plan_create_t(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, const uint32_t *bins,
+                  const float *pooling, bool per_stack, void *stream, PlanImpl **out)
 {
     if (!out) return LSCOMP_ERR_ARG;
     *out = nullptr;
-    if (!ws || !stacks || n == 0) return LSCOMP_ERR_ARG;
+    if (!ws || !stacks || n == 0 || !bins || !pooling) return LSCOMP_ERR_ARG;
     // one ordinary call first: it checks every argument, tunes the key when
     // tuning is on, and leaves the streams written
-    int r = n == 1 ? compress_async_t_dispatch<T>(ws, stacks[0], bins, pooling, stream)
-                   : compress_batch_t<T>(ws, stacks, n, bins, pooling, nullptr, nullptr, stream);
+    int r = n == 1 ? compress_async_t_dispatch<T>(ws, stacks[0], bins, pooling[0], stream)
+                   : compress_batch_t<T>(ws, stacks, n, bins, pooling, per_stack, nullptr, nullptr, stream);
     if (!r && n == 1) r = lscomp_workspace_check(ws, stream);
     if (r) return r;
-    Codec c;
+    std::vector<Codec> codec;
     int layout = 0;
-    make_codec(bins, pooling, sizeof(T) == 4, c, layout);
-    const bool pool = c.pool_min <= 64;
+    bool pool = false;
+    batch_codecs(bins, pooling, per_stack, n, sizeof(T) == 4, codec, layout, pool);
+    const Codec &c = codec[0];
     int vec = 16;
     for (uint32_t s = 0; s < n; s++) {
         const int v = vec_class(stacks[s].d_in, stacks[s].z, sizeof(T));
@@ -292,6 +326,7 @@ int plan_create_t(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, 
         std::vector<BatchStack> h(n);
         for (uint32_t s = 0; s < n; s++) {
             h[s].g = geom[s];
+            h[s].c = codec[s];
             h[s].in = stacks[s].d_in;
             h[s].out = stacks[s].d_out;
             h[s].cap = stacks[s].cap;
@@ -388,25 +423,49 @@ extern "C" {
 int lscomp_compress_batch_u16(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, const uint32_t bins[4],
                               float pooling, uint64_t *stream_len, uint64_t *ref_size, void *stream)
 {
-    return compress_batch_t<uint16_t>(ws, stacks, n, bins, pooling, stream_len, ref_size, stream);
+    return compress_batch_t<uint16_t>(ws, stacks, n, bins, &pooling, false, stream_len, ref_size, stream);
 }
 
 int lscomp_compress_batch_u32(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, const uint32_t bins[4],
                               float pooling, uint64_t *stream_len, uint64_t *ref_size, void *stream)
 {
-    return compress_batch_t<uint32_t>(ws, stacks, n, bins, pooling, stream_len, ref_size, stream);
+    return compress_batch_t<uint32_t>(ws, stacks, n, bins, &pooling, false, stream_len, ref_size, stream);
+}
+
+int lscomp_compress_batch_ex_u16(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, const uint32_t *bins,
+                                 const float *pooling, uint64_t *stream_len, uint64_t *ref_size, void *stream)
+{
+    return compress_batch_t<uint16_t>(ws, stacks, n, bins, pooling, true, stream_len, ref_size, stream);
+}
+
+int lscomp_compress_batch_ex_u32(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, const uint32_t *bins,
+                                 const float *pooling, uint64_t *stream_len, uint64_t *ref_size, void *stream)
+{
+    return compress_batch_t<uint32_t>(ws, stacks, n, bins, pooling, true, stream_len, ref_size, stream);
 }
 
 int lscomp_plan_create_u16(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, const uint32_t bins[4],
                            float pooling, void *stream, lscomp_plan **plan)
 {
-    return plan_create_t<uint16_t>(ws, stacks, n, bins, pooling, stream, reinterpret_cast<PlanImpl **>(plan));
+    return plan_create_t<uint16_t>(ws, stacks, n, bins, &pooling, false, stream, reinterpret_cast<PlanImpl **>(plan));
 }
 
 int lscomp_plan_create_u32(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, const uint32_t bins[4],
                            float pooling, void *stream, lscomp_plan **plan)
 {
-    return plan_create_t<uint32_t>(ws, stacks, n, bins, pooling, stream, reinterpret_cast<PlanImpl **>(plan));
+    return plan_create_t<uint32_t>(ws, stacks, n, bins, &pooling, false, stream, reinterpret_cast<PlanImpl **>(plan));
+}
+
+int lscomp_plan_create_ex_u16(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, const uint32_t *bins,
+                              const float *pooling, void *stream, lscomp_plan **plan)
+{
+    return plan_create_t<uint16_t>(ws, stacks, n, bins, pooling, true, stream, reinterpret_cast<PlanImpl **>(plan));
+}
+
+int lscomp_plan_create_ex_u32(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, const uint32_t *bins,
+                              const float *pooling, void *stream, lscomp_plan **plan)
+{
+    return plan_create_t<uint32_t>(ws, stacks, n, bins, pooling, true, stream, reinterpret_cast<PlanImpl **>(plan));
 }
 
 int lscomp_plan_run(lscomp_plan *plan, void *stream, uint64_t *stream_len, uint64_t *ref_size)

@@ -135,9 +135,12 @@ struct EncArgs {
 
 // One stack of a batch launch (device memory).  Its tiles are the tiles
 // tile0 .. tile0 + g.ntiles - 1 of the batch; sizes receives
-// {stream_len, payload} when its last tile is written.
+// {stream_len, payload} when its last tile is written.  Stacks of one launch
+// may have different bins and pooling thresholds: the launch is instantiated
+// for a bins layout that covers all of them.
 struct BatchStack {
     Geom g;
+    Codec c;  // the stack's bins and pooling threshold
     const void *in;
     uint8_t *out;
     unsigned long long cap;
@@ -646,6 +649,8 @@ struct EncSmem {
     uint64_t in_full2[kInStages];
     // batch launches: the stack of each input slot and of each payload slot
     Geom in_geom[kInStages];
+    Codec in_codec[kInStages];
+    Codec grp_codec[kMaxGroups];   // per compute group: its tile's codec, for pass B
     const BatchStack *in_stack[kInStages];
     uint8_t *in_out[kInStages];
     unsigned long long in_gtile[kInStages];   // tile index over the batch (look-back state)
@@ -1082,6 +1087,14 @@ __device__ __forceinline__ void enc_compute(const EncArgs<T> &a, EncSmem &sm)
         uint8_t *const out = BATCH ? sm.in_out[i] : a.out;
         const BatchStack *const bstack = BATCH ? sm.in_stack[i] : nullptr;
         const unsigned long long gt = BATCH ? sm.in_gtile[i] : t;  // look-back state of the tile
+        const Codec &cA = BATCH ? sm.in_codec[i] : a.c;             // pass A reads the slot's codec
+        const Codec &cB = BATCH ? sm.grp_codec[grp] : a.c;          // pass B the group's copy
+        if (BATCH) {
+            constexpr uint32_t kCWords = sizeof(Codec) / 4;
+            if (gtid < kCWords)
+                reinterpret_cast<uint32_t *>(&sm.grp_codec[grp])[gtid] =
+                    reinterpret_cast<const uint32_t *>(&sm.in_codec[i])[gtid];
+        }
         const TileInfo ti = tile_info(g, t);
         const uint8_t *stage = sm.in[i];
 
@@ -1100,7 +1113,7 @@ __device__ __forceinline__ void enc_compute(const EncArgs<T> &a, EncSmem &sm)
                 SegLoc L = seg_locate<T, true>(g, ti, sm.br_rel[i], sm.br_rows[i], stage, sm.in_mis[i], active ? b : 0, r);
                 load_rows<T, VEC>(L, active, r, A[q], B[q]);
                 uint32_t rb;
-                hq[q] = block_header<T, BINS == BINS_IDENT ? BINS_EQUAL : BINS, POOL, BINS == BINS_IDENT>(A[q], B[q], a.c, rb);
+                hq[q] = block_header<T, BINS == BINS_IDENT ? BINS_EQUAL : BINS, POOL, BINS == BINS_IDENT>(A[q], B[q], cA, rb);
                 if (active && r == 0) {
                     hdr[b] = (uint8_t)hq[q];
                     bad |= rb;
@@ -1137,7 +1150,7 @@ __device__ __forceinline__ void enc_compute(const EncArgs<T> &a, EncSmem &sm)
             if (u < nunits) {
                 const uint32_t b = u * 8 + jb;
                 const bool active = b < ti.nblk;
-                block_pack<T, BINS == BINS_IDENT>(A[q], B[q], hq[q], active, r, xs, a.c,
+                block_pack<T, BINS == BINS_IDENT>(A[q], B[q], hq[q], active, r, xs, cB,
                                                    st + (active ? off[b] : 0u));
             }
         }
@@ -1169,6 +1182,11 @@ __device__ __forceinline__ unsigned long long batch_slot(const EncArgs<T> &a, En
     const uint32_t *src = reinterpret_cast<const uint32_t *>(&st->g);
     uint32_t *dst = reinterpret_cast<uint32_t *>(&sm.in_geom[s]);
     for (uint32_t w = lane; w < kWords; w += 32) dst[w] = src[w];
+    constexpr uint32_t kCWords = sizeof(Codec) / 4;
+    static_assert(sizeof(Codec) % 4 == 0, "codec copied in words");
+    const uint32_t *csrc = reinterpret_cast<const uint32_t *>(&st->c);
+    uint32_t *cdst = reinterpret_cast<uint32_t *>(&sm.in_codec[s]);
+    for (uint32_t w = lane; w < kCWords; w += 32) cdst[w] = csrc[w];
     if (lane == 0) {
         sm.in_stack[s] = st;
         sm.in_out[s] = st->out;

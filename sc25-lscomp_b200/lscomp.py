@@ -131,6 +131,12 @@ def load_library() -> ctypes.CDLL:
                                                                  pu64, pu64, vp]
         getattr(lib, f"lscomp_plan_create_{sfx}").argtypes = [vp, ctypes.POINTER(LscompStack), u32, bins_t, f32, vp,
                                                               ctypes.POINTER(vp)]
+        getattr(lib, f"lscomp_compress_batch_ex_{sfx}").argtypes = [vp, ctypes.POINTER(LscompStack), u32,
+                                                                    ctypes.POINTER(u32), ctypes.POINTER(f32),
+                                                                    pu64, pu64, vp]
+        getattr(lib, f"lscomp_plan_create_ex_{sfx}").argtypes = [vp, ctypes.POINTER(LscompStack), u32,
+                                                                 ctypes.POINTER(u32), ctypes.POINTER(f32), vp,
+                                                                 ctypes.POINTER(vp)]
     lib.lscomp_plan_run.argtypes = [vp, vp, pu64, pu64]
     lib.lscomp_plan_destroy.argtypes = [vp]
     lib.lscomp_tune_mode.argtypes = [ctypes.c_int]
@@ -227,6 +233,50 @@ def compress_into(ws: Workspace, d_in, dims, bins, pooling: float, d_out, stream
     return int(sl.value), int(rs.value)
 
 
+def _stack_array(items):
+    n = len(items)
+    sfx = _suffix(items[0][0])
+    arr = (LscompStack * n)()
+    for i, it in enumerate(items):
+        d_in, dims, d_out = it[0], it[1], it[2]
+        if _suffix(d_in) != sfx:
+            raise ValueError("a batch holds one element type")
+        x, y, z = (int(v) for v in dims)
+        arr[i] = LscompStack(d_in.data_ptr(), x, y, z, d_out.data_ptr(), d_out.numel() * d_out.element_size())
+    return sfx, arr
+
+
+def _per_stack_settings(items):
+    n = len(items)
+    bins = (ctypes.c_uint32 * (4 * n))()
+    pool = (ctypes.c_float * n)()
+    for i, it in enumerate(items):
+        b, p = it[3], it[4]
+        for k in range(4):
+            bins[4 * i + k] = int(b[k])
+        pool[i] = float(p)
+    return bins, pool
+
+
+def compress_batch_mixed(ws: Workspace, items, stream=None):
+    """Compress many stacks in one launch, each with its own settings:
+    items = [(d_in, dims, d_out, bins, pooling), ...] (one element type).
+    Returns [(stream_len, ref_size), ...]; each stream is the one
+    compress_into writes for that stack alone with its settings."""
+    lib = load_library()
+    n = len(items)
+    if n == 0:
+        return []
+    sfx, arr = _stack_array(items)
+    bins, pool = _per_stack_settings(items)
+    sl = (ctypes.c_uint64 * n)()
+    rs = (ctypes.c_uint64 * n)()
+    st = getattr(lib, f"lscomp_compress_batch_ex_{sfx}")(ws.handle, arr, n, bins, pool, sl, rs,
+                                                         ctypes.c_void_p(_stream_handle(stream)))
+    _check(st, f"lscomp_compress_batch_ex_{sfx}")
+    return [(int(sl[i]), int(rs[i])) for i in range(n)]
+
+
 def compress_batch(ws: Workspace, items, bins, pooling: float, stream=None):
     """Compress many stacks in one launch: items = [(d_in, dims, d_out), ...],
     all uint16 (int16 tensors) or all uint32 (int32 tensors), with the same
@@ -257,26 +307,27 @@ class Plan:
     run() on new contents of the same buffers.  Creating it runs one ordinary
     call through ws (the streams are written)."""
 
-    def __init__(self, ws: Workspace, items, bins, pooling: float, stream=None):
+    def __init__(self, ws: Workspace, items, bins=None, pooling: Optional[float] = None, stream=None):
+        """items = [(d_in, dims, d_out), ...] with bins and pooling for all,
+        or [(d_in, dims, d_out, bins, pooling), ...] with bins=None."""
         lib = load_library()
         self._lib = lib
         self.handle = None
         n = len(items)
         if n == 0:
             raise ValueError("a plan holds at least one stack")
-        sfx = _suffix(items[0][0])
-        arr = (LscompStack * n)()
-        for i, (d_in, dims, d_out) in enumerate(items):
-            if _suffix(d_in) != sfx:
-                raise ValueError("a plan holds one element type")
-            x, y, z = (int(v) for v in dims)
-            arr[i] = LscompStack(d_in.data_ptr(), x, y, z, d_out.data_ptr(), d_out.numel() * d_out.element_size())
+        sfx, arr = _stack_array(items)
         self.n = n
         self._keep = items  # the buffers must outlive the plan
         h = ctypes.c_void_p()
-        _check(getattr(lib, f"lscomp_plan_create_{sfx}")(ws.handle, arr, n, _bins(bins), ctypes.c_float(pooling),
-                                                         ctypes.c_void_p(_stream_handle(stream)), ctypes.byref(h)),
-               f"lscomp_plan_create_{sfx}")
+        hs = ctypes.c_void_p(_stream_handle(stream))
+        if bins is None:
+            pb, pp = _per_stack_settings(items)
+            st = getattr(lib, f"lscomp_plan_create_ex_{sfx}")(ws.handle, arr, n, pb, pp, hs, ctypes.byref(h))
+        else:
+            st = getattr(lib, f"lscomp_plan_create_{sfx}")(ws.handle, arr, n, _bins(bins), ctypes.c_float(pooling),
+                                                           hs, ctypes.byref(h))
+        _check(st, f"lscomp_plan_create_{sfx}")
         self.handle = h
 
     def run(self, stream=None):

@@ -151,3 +151,72 @@ def test_batch_errors(lz, ws):
     with pytest.raises(lz.LscompError) as e:
         lz.compress_batch(ws, [(d, (2, 64, 0), good)], *LOSSLESS)
     assert e.value.status == 1
+
+
+SETTINGS = [((1, 1, 1, 1), 1.0), ((3, 5, 10, 15), 0.3), ((3, 5, 10, 15), 0.5), ((5, 10, 15, 20), 0.8),
+            ((1, 1, 1, 1), 0.5), ((7, 7, 7, 7), 0.8)]
+
+
+@pytest.mark.parametrize("with_general", [False, True])
+def test_mixed_settings_u16(lz, ws, oracle, with_general):
+    # every stack with its own bins and threshold, one launch: increasing-bins
+    # kernel for the monotone mix, the general kernel once a stack's bins
+    # do not increase
+    rng = np.random.default_rng(11)
+    settings = SETTINGS + ([GENERAL] if with_general else [])
+    shapes = SHAPES + [(3, 130, 150), (2, 300, 210)]
+    items, arrays, chosen = [], [], []
+    for i, dims in enumerate(shapes):
+        a = stack16(dims, seed=300 + i)
+        b, p = settings[int(rng.integers(0, len(settings)))] if i >= len(settings) else settings[i]
+        d_in = torch.from_numpy(a.view(np.int16).ravel()).cuda()
+        out = torch.full((lz.max_stream_bytes(dims),), 0xAB, dtype=torch.uint8, device="cuda")
+        items.append((d_in, dims, out, b, p))
+        arrays.append(a)
+        chosen.append((b, p))
+    res = lz.compress_batch_mixed(ws, items)
+    for (d_in, dims, out, b, p), a, (sl, rs) in zip(items, arrays, res):
+        ref, sl1, rs1 = single(lz, ws, d_in, dims, b, p, 2)
+        assert (sl, rs) == (sl1, rs1), (dims, b, p)
+        assert np.array_equal(out[:sl].cpu().numpy(), ref), (dims, b, p)
+        s_o, _ = oracle.compress(a, dims, b, p)
+        assert np.array_equal(ref, np.asarray(s_o)), (dims, b, p)
+
+
+def test_mixed_settings_u32(lz, ws):
+    shapes = [(1, 8, 8), (2, 13, 21), (3, 37, 53), (2, 17, 1100), (4, 64, 64)]
+    items = []
+    for i, dims in enumerate(shapes):
+        b, p = SETTINGS[i % len(SETTINGS)]
+        d_in = torch.from_numpy(stack32(dims, seed=400 + i).view(np.int32).ravel()).cuda()
+        out = torch.zeros(lz.max_stream_bytes(dims, 4), dtype=torch.uint8, device="cuda")
+        items.append((d_in, dims, out, b, p))
+    res = lz.compress_batch_mixed(ws, items)
+    for (d_in, dims, out, b, p), (sl, rs) in zip(items, res):
+        ref, sl1, rs1 = single(lz, ws, d_in, dims, b, p, 4)
+        assert (sl, rs) == (sl1, rs1), (dims, b, p)
+        assert np.array_equal(out[:sl].cpu().numpy(), ref), (dims, b, p)
+
+
+def test_mixed_settings_plan(lz, ws):
+    shapes = [(2, 100, 130), (1, 9, 2049), (5, 31, 7), (4, 64, 64), (3, 37, 53)]
+    items = []
+    for i, dims in enumerate(shapes):
+        b, p = SETTINGS[(i + 1) % len(SETTINGS)]
+        d_in = torch.from_numpy(stack16(dims, seed=500 + i).view(np.int16).ravel()).cuda()
+        out = torch.zeros(lz.max_stream_bytes(dims), dtype=torch.uint8, device="cuda")
+        items.append((d_in, dims, out, b, p))
+    plan = lz.Plan(ws, items)
+    try:
+        for rnd in range(2):
+            if rnd:
+                for i, (d_in, dims, out, b, p) in enumerate(items):
+                    d_in.copy_(torch.from_numpy(stack16(dims, seed=600 + i).view(np.int16).ravel()).cuda())
+                    out.fill_(0xCD)
+            res = plan.run()
+            for (d_in, dims, out, b, p), (sl, rs) in zip(items, res):
+                ref, sl1, rs1 = single(lz, ws, d_in, dims, b, p, 2)
+                assert (sl, rs) == (sl1, rs1), (rnd, dims)
+                assert np.array_equal(out[:sl].cpu().numpy(), ref), (rnd, dims)
+    finally:
+        plan.close()
