@@ -306,6 +306,12 @@ int lscomp_quality_u16(const uint16_t *d_ori, const uint16_t *d_dec, uint32_t x,
 int lscomp_quality_u32(const uint32_t *d_ori, const uint32_t *d_dec, uint32_t x, uint32_t y, uint32_t z,
                        double psnr[6], double *ssim, void *stream);
 
+/* allow = 0: calls through this workspace never run the launch-configuration
+   tuner (they use its table, else the built-in rules) -- for latency-bound
+   loops such as the serving loop, whose requests must not wait for a tuning
+   run; allow = 1 (the default) restores tuning. */
+int lscomp_workspace_set_tuning(lscomp_workspace *ws, int allow);
+
 /* Wait for the workspace's last launch on `stream` and return its status. */
 int lscomp_workspace_check(lscomp_workspace *ws, void *stream);
 

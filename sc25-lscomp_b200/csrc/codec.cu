@@ -218,6 +218,14 @@ int lscomp_workspace_destroy(lscomp_workspace *ws)
     return LSCOMP_OK;
 }
 
+int lscomp_workspace_set_tuning(lscomp_workspace *ws, int allow)
+{
+    if (!ws) return LSCOMP_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ws->mu);
+    ws->no_tune = allow == 0;
+    return LSCOMP_OK;
+}
+
 int lscomp_workspace_check(lscomp_workspace *ws, void *stream)
 {
     if (!ws) return LSCOMP_ERR_ARG;

@@ -28,6 +28,7 @@ struct lscomp_workspace {
     uint32_t stacks_cap = 0;
     uint32_t *d_tile_stack = nullptr;
     uint64_t tile_stack_cap = 0;
+    bool no_tune = false;              // calls through this workspace never tune
     std::mutex mu;
 };
 
@@ -318,7 +319,7 @@ inline TuneCfg tune_choose(lscomp_workspace *ws, const TuneKey &key, const TuneC
 {
     TuneCfg c;
     if (tune_lookup(key, c)) return c;
-    if (!may_tune || !tune_mode()) return rule;
+    if (!may_tune || ws->no_tune || !tune_mode()) return rule;
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return rule;
     cudaEvent_t e0 = nullptr, e1 = nullptr;

@@ -12,9 +12,9 @@
 //     their footprints fit the arena, so the device never runs out of memory
 //     however the load arrives, and a request larger than the whole arena is
 //     refused (LSCOMP_ERR_TOO_LARGE);
-//   * continuous batching: the compress requests of a round that share
-//     element type, bins and pooling threshold go to the GPU as one batch
-//     launch (lscomp_compress_batch_*), whatever their shapes; decompress
+//   * continuous batching: the compress requests of a round of one element
+//     type go to the GPU as one batch launch (lscomp_compress_batch_ex_*),
+//     whatever their shapes, bins and pooling thresholds; decompress
 //     requests of the round run one after the other;
 //   * staging: inputs and outputs pass through pinned host memory of the
 //     arena's size, so the device copies run at full link speed from
@@ -187,7 +187,8 @@ void run_round(lscomp_server *s, std::vector<Request *> &round)
                             s->st) != cudaSuccess)
             st[i] = LSCOMP_ERR_CUDA;
     }
-    // compress groups (same element type, bins, pooling): one batch launch each
+    // compress requests of one element type: one batch launch, each stack
+    // with its own bins and pooling threshold
     std::vector<bool> taken(round.size(), false);
     for (size_t i = 0; i < round.size(); i++) {
         Request *r = round[i];
@@ -195,13 +196,14 @@ void run_round(lscomp_server *s, std::vector<Request *> &round)
         std::vector<size_t> grp;
         for (size_t j = i; j < round.size(); j++) {
             Request *q = round[j];
-            if (!taken[j] && q->op == 0 && !st[j] && q->eb == r->eb && q->p == r->p &&
-                memcmp(q->bins, r->bins, sizeof(r->bins)) == 0) {
+            if (!taken[j] && q->op == 0 && !st[j] && q->eb == r->eb) {
                 grp.push_back(j);
                 taken[j] = true;
             }
         }
         std::vector<lscomp_stack> stacks(grp.size());
+        std::vector<uint32_t> bins(4 * grp.size());
+        std::vector<float> pool(grp.size());
         std::vector<uint64_t> len(grp.size()), ref(grp.size());
         for (size_t g = 0; g < grp.size(); g++) {
             const size_t j = grp[g];
@@ -211,11 +213,13 @@ void run_round(lscomp_server *s, std::vector<Request *> &round)
             stacks[g].z = round[j]->z;
             stacks[g].d_out = s->arena + out_off[j] + kHdr;
             stacks[g].cap = round[j]->out_dev - kHdr;
+            memcpy(&bins[4 * g], round[j]->bins, sizeof(round[j]->bins));
+            pool[g] = round[j]->p;
         }
-        const int b = r->eb == 2 ? lscomp_compress_batch_u16(s->ws, stacks.data(), (uint32_t)grp.size(), r->bins,
-                                                             r->p, len.data(), ref.data(), s->st)
-                                 : lscomp_compress_batch_u32(s->ws, stacks.data(), (uint32_t)grp.size(), r->bins,
-                                                             r->p, len.data(), ref.data(), s->st);
+        const int b = r->eb == 2 ? lscomp_compress_batch_ex_u16(s->ws, stacks.data(), (uint32_t)grp.size(),
+                                                                bins.data(), pool.data(), len.data(), ref.data(), s->st)
+                                 : lscomp_compress_batch_ex_u32(s->ws, stacks.data(), (uint32_t)grp.size(),
+                                                                bins.data(), pool.data(), len.data(), ref.data(), s->st);
         s->batches++;
         s->batched_requests += grp.size();
         for (size_t g = 0; g < grp.size(); g++) {
@@ -329,6 +333,10 @@ int lscomp_server_create(lscomp_server **out, int device, uint64_t arena_bytes)
     s->device = dev;
     s->arena_bytes = arena_bytes;
     int st = lscomp_workspace_create(&s->ws, dev);
+    // no request waits for a tuning run: the server's calls use the tuner's
+    // table when it has the key (lscomp_tune_load at start-up) and the
+    // built-in rules otherwise
+    if (!st) st = lscomp_workspace_set_tuning(s->ws, 0);
     if (!st && cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) != cudaSuccess) st = LSCOMP_ERR_CUDA;
     if (!st && cudaMalloc(&s->arena, arena_bytes) != cudaSuccess) st = LSCOMP_ERR_NOMEM;
     if (!st && cudaMallocHost(&s->staging, arena_bytes) != cudaSuccess) st = LSCOMP_ERR_NOMEM;

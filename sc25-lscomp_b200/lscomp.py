@@ -100,6 +100,7 @@ def load_library() -> ctypes.CDLL:
     lib.lscomp_workspace_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int]
     lib.lscomp_workspace_destroy.argtypes = [vp]
     lib.lscomp_workspace_check.argtypes = [vp, vp]
+    lib.lscomp_workspace_set_tuning.argtypes = [vp, ctypes.c_int]
     lib.lscomp_compress_u16.argtypes = [vp, vp, u32, u32, u32, bins_t, f32, vp, u64, pu64, pu64, vp]
     lib.lscomp_compress_u16_async.argtypes = [vp, vp, u32, u32, u32, bins_t, f32, vp, u64, vp, vp]
     lib.lscomp_decompress_u16.argtypes = [vp, vp, u64, u32, u32, u32, bins_t, f32, vp, vp]
@@ -186,6 +187,10 @@ class Workspace:
     @property
     def handle(self):
         return self._ws
+
+    def set_tuning(self, allow: bool) -> None:
+        """False: calls through this workspace never run the tuner."""
+        _check(load_library().lscomp_workspace_set_tuning(self._ws, 1 if allow else 0), "lscomp_workspace_set_tuning")
 
     def close(self):
         if self._ws:

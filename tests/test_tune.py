@@ -268,3 +268,26 @@ def test_plan_rejects_bad_arguments(lz, ws):
         lz.Plan(ws, [(d_in, dims, small)], *LOSSY)
     with pytest.raises(ValueError):
         lz.Plan(ws, [], *LOSSY)
+
+
+@pytest.mark.gpu
+def test_workspace_without_tuning(lz, oracle):
+    prev = lz.tune_mode(1)
+    ws2 = lz.Workspace(0)
+    try:
+        lz.tune_clear()
+        ws2.set_tuning(False)
+        dims = (64, 256, 1024)
+        a = random_stack(dims, seed=9)
+        out = torch.zeros(lz.max_stream_bytes(dims), dtype=torch.uint8, device="cuda")
+        sl, _ = lz.compress_into(ws2, to_dev(a), dims, *LOSSLESS, out)
+        assert lz.tune_table() == []
+        s_o, _ = oracle.compress(a, dims, *LOSSLESS)
+        assert np.array_equal(out[:sl].cpu().numpy(), s_o)
+        ws2.set_tuning(True)
+        lz.compress_into(ws2, to_dev(a), dims, *LOSSLESS, out)
+        assert len(lz.tune_table()) == 1
+    finally:
+        ws2.close()
+        lz.tune_clear()
+        lz.tune_mode(prev)
