@@ -11,13 +11,17 @@ four passes over the stack.
     e2e    = the same metric through the C ABI with host buffers: every pass
              copies its input from pinned host memory and its result back;
     roofline  = the dominant kernel's algorithmic bytes per launch / its mean
-             launch time, against MEASURED_PEAKS.json hbm_gbs;
+             launch time, against the measured HBM copy bandwidth of this
+             pool's B200s;
     cpu_baseline = the C/OpenMP oracle on a bounded frame sample, all cores.
 
 --impl reference times the reference's own CUDA build (oracle/_ref) through
-its host API on the same stack and steps.  --gpus N (torchrun) runs N
-independent replicas, one per GPU: the codec does not shard, so there is no
-data-path collective; the step time is the max over ranks.
+its host API on the same stack and steps (e2e: the same host-buffer path as
+this library's e2e); --impl reference --ref-cpu times the path on the host
+cores instead (the reference has no CPU implementation, so the C/OpenMP
+oracle, all threads, a bounded frame sample per step).  --gpus N (torchrun) runs N independent
+replicas, one per GPU: the codec does not shard, so there is no data-path
+collective; the step time is the max over ranks.
 """
 import argparse
 import json
@@ -53,6 +57,10 @@ def parse():
                     help="serving benchmark: Poisson arrivals at this many requests per second (its own JSON line)")
     ap.add_argument("--serve-seconds", type=float, default=10.0)
     ap.add_argument("--batch-frames", type=int, default=16, help="largest frame count of a batch stack")
+    ap.add_argument("--ref-cpu", action="store_true",
+                    help="with --impl reference: the oracle on the host cores instead of the reference's CUDA build")
+    ap.add_argument("--ref-step-seconds", type=float, default=1.5,
+                    help="with --impl reference: CPU time of one step's sample")
     ap.add_argument("--batch", type=int, default=0,
                     help="batched-stacks benchmark over this many stacks (its own JSON line)")
     return ap.parse_args()
@@ -671,9 +679,17 @@ def bench_e2e(args, dims, ws, h, dev, nbytes, sizes, world):
 
 
 def bench_reference(args, dims, rank, world, dev, d_in, d_cmp, d_dec, nbytes, config, h):
-    """The reference's own CUDA build through its host API
-    (cuLSZ_compression_uint16_bsize64 / cuLSZ_decompression_uint16_bsize64),
-    timed like the reference CLI times it: the whole host call."""
+    """The reference arm.  Default: the reference's own CUDA build (sm_100a)
+    through its host API (cuLSZ_compression_uint16_bsize64 /
+    cuLSZ_decompression_uint16_bsize64) on the same stack and steps: value
+    with the stack resident in HBM, timed like the reference CLI times it
+    (the whole host call); e2e through host buffers with every pass's input
+    and output copied across PCIe, as the reference CLI moves them and as
+    this library's e2e does.  --ref-cpu: the path on the host cores -- the
+    reference has no CPU implementation of the codec, so the oracle (the same
+    algorithm in C/OpenMP, streams byte-identical to the reference build's)
+    with every host thread, each step one pass over a bounded sample of the
+    stack's first frames."""
     import torch
 
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -684,13 +700,72 @@ def bench_reference(args, dims, rank, world, dev, d_in, d_cmp, d_dec, nbytes, co
         dist.barrier()
         dist.destroy_process_group()
         return
+    if args.ref_cpu:
+        out = bench_reference_cpu(args, dims, config)
+    else:
+        out = bench_reference_gpu(args, dims, dev, d_in, d_cmp, d_dec, nbytes, config, h)
+    print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def bench_reference_cpu(args, dims, config):
+    import lscomp
+    from oracle import Oracle
+
+    orc = Oracle()
+    threads = orc.max_threads()
+    x, y, z = dims
+
+    def sample(nf):
+        return getattr(lscomp, "synth_cssi")(dims, seed=SEED, frames=(0, nf))
+
+    def step(a, nf):
+        d = (nf, y, z)
+        t0 = time.perf_counter()
+        for _, bins, p in MODES:
+            s, _ = orc.compress(a, d, bins, p, threads=threads)
+            orc.decompress(s, d, bins, p, threads=threads)
+        return time.perf_counter() - t0
+
+    # size the sample so one step takes about args.ref_step_seconds
+    nf = 2
+    t = step(sample(nf), nf)
+    nf = max(1, min(x, int(nf * args.ref_step_seconds / max(t, 1e-3))))
+    a = sample(nf)
+    for _ in range(max(args.warmup, 3)):
+        step(a, nf)
+    ts = [step(a, nf) for _ in range(args.steps)]
+    sec = float(np.mean(ts))
+    sbytes = a.size * 2
+    value = 4 * sbytes / sec / 1e9
+    smp = (f"first {nf} of {x} frames ({sbytes / 1e9:.3f} GB) of the same CSSI-like stack per step, lossless + "
+           f"lossy compress + decompress, {sec:.2f} s per step")
+    return {"impl": "reference",
+            "metric": "lsCOMP compress+decompress throughput (lossless and lossy b=3 5 10 15 p=0.5), "
+                      "uncompressed GB per second",
+            "value": round(value, 3), "unit": "GB/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": round(sec * 1e3, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic (seeded CSSI-like generator)",
+            "config": config,
+            "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": threads, "kind": "port",
+                             "sample": smp + "; the reference has no CPU implementation, so the oracle (its "
+                                             "algorithm restated in C/OpenMP, byte-identical streams) runs"},
+            "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def bench_reference_gpu(args, dims, dev, d_in, d_cmp, d_dec, nbytes, config, h):
+    import torch
+
     try:
         from oracle import REF_LIB, RefLib
 
         ref = RefLib(REF_LIB)
     except Exception as e:  # the reference build is not present
-        print(json.dumps({"impl": "reference", "unavailable": f"reference build missing: {e}"}))
-        return
+        return {"impl": "reference", "unavailable": f"reference build missing: {e}"}
     sizes = {}
     for name, bins, p in MODES:
         d_cmp.zero_()
@@ -717,23 +792,52 @@ def bench_reference(args, dims, rank, world, dev, d_in, d_cmp, d_dec, nbytes, co
     clk = clocks.stop()
     ms = e0.elapsed_time(e1) / args.steps
     value = 4 * nbytes / (ms / 1e3) / 1e9
-    out = {"impl": "reference",
-           "metric": "lsCOMP compress+decompress throughput (lossless and lossy b=3 5 10 15 p=0.5), "
-                     "uncompressed GB per second",
-           "value": round(value, 2), "unit": "GB/s", "n_gpus": 1, "steps": args.steps,
-           "warmup": max(args.warmup, 3), "ms_per_step": round(ms, 4), "higher_is_better": True,
-           "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic (seeded CSSI-like generator)",
-           "config": config, "clocks": clk,
-           "cpu_baseline": {"value": round(value, 2), "unit": "GB/s", "cores": 1, "kind": "reference",
-                            "sample": "the reference's CUDA sources (nvcc -O3 sm_100a) through its host API on the "
-                                      "full stack; the reference has no CPU implementation"},
-           "e2e": {"value": round(value, 2), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(out), flush=True)
-    if world > 1:
-        import torch.distributed as dist
+    e2e = None
+    if args.e2e_steps > 0:
+        # host buffers in and out, as the reference CLI moves them: stack to
+        # the device, compress, stream back; stream to the device,
+        # decompress, stack back (pinned host memory, like this library's e2e)
+        h_in = torch.from_numpy(h.view(np.int16)).pin_memory()
+        h_out = torch.empty_like(h_in).pin_memory()
+        h_cmp = torch.empty(max(sizes.values()), dtype=torch.uint8).pin_memory()
+        moved = {"h2d": 0, "d2h": 0}
 
-        dist.barrier()
-        dist.destroy_process_group()
+        def step_e2e():
+            moved["h2d"] = moved["d2h"] = 0
+            for name, bins, p in MODES:
+                d_in.copy_(h_in, non_blocking=True)
+                sl = ref.compress(d_in.data_ptr(), d_cmp.data_ptr(), dims, bins, p)
+                h_cmp[:sl].copy_(d_cmp[:sl], non_blocking=True)
+                d_cmp[:sl].copy_(h_cmp[:sl], non_blocking=True)
+                ref.decompress(d_dec.data_ptr(), d_cmp.data_ptr(), sl, dims, bins, p)
+                h_out.copy_(d_dec, non_blocking=True)
+                moved["h2d"] += nbytes + sl
+                moved["d2h"] += sl + nbytes
+            torch.cuda.synchronize()
+
+        step_e2e()
+        e0.record(stream)
+        for _ in range(args.e2e_steps):
+            step_e2e()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ems = e0.elapsed_time(e1) / args.e2e_steps
+        e2e = {"value": round(4 * nbytes / (ems / 1e3) / 1e9, 2), "unit": "GB/s",
+               "h2d_bytes_per_step": int(moved["h2d"]), "d2h_bytes_per_step": int(moved["d2h"]),
+               "ms_per_step": round(ems, 3),
+               "path": "reference host API (cuLSZ_*_bsize64) with pinned host buffers copied in and out"}
+    return {"impl": "reference",
+            "metric": "lsCOMP compress+decompress throughput (lossless and lossy b=3 5 10 15 p=0.5), "
+                      "uncompressed GB per second",
+            "value": round(value, 2), "unit": "GB/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": round(ms, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic (seeded CSSI-like generator)",
+            "config": config, "clocks": clk,
+            "cpu_baseline": {"value": round(value, 2), "unit": "GB/s", "cores": 1, "kind": "reference",
+                             "sample": "the reference's CUDA sources (nvcc -O3 sm_100a) through its host API on the "
+                                       "full stack; the reference has no CPU implementation (bench.py --impl "
+                                       "reference --ref-cpu times the C/OpenMP oracle on the host cores)"},
+            "e2e": e2e}
 
 
 if __name__ == "__main__":
