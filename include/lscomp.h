@@ -110,6 +110,30 @@ int lscomp_decompress_u32_async(lscomp_workspace *ws, const uint8_t *d_in, uint6
                                 uint32_t y, uint32_t z, const uint32_t bins[4], float pooling,
                                 uint32_t *d_out, void *stream);
 
+/* Compression and decompression from and to HOST memory (the reference's
+   CLI does this with one blocking copy each way around the device call).
+   The stack moves through the device in chunks of whole frames (about
+   128 MB each) on two copy streams, so copies up, kernels and copies down
+   of different chunks overlap; the stream (h_out, cap bytes) and the
+   decoded stack are exactly those of the device-memory calls.  Pinned host
+   buffers (cudaMallocHost / cudaHostRegister) let the copies overlap;
+   pageable ones work but copy synchronously.  The workspace keeps the copy
+   streams and four chunk buffers (about 0.5 GB for uint16) for later
+   calls.  Synchronous: returns when every byte is in place. */
+int lscomp_compress_host_u16(lscomp_workspace *ws, const uint16_t *h_in, uint32_t x, uint32_t y, uint32_t z,
+                             const uint32_t bins[4], float pooling, uint8_t *h_out, uint64_t cap,
+                             uint64_t *stream_len, uint64_t *ref_size, void *stream);
+int lscomp_compress_host_u32(lscomp_workspace *ws, const uint32_t *h_in, uint32_t x, uint32_t y, uint32_t z,
+                             const uint32_t bins[4], float pooling, uint8_t *h_out, uint64_t cap,
+                             uint64_t *stream_len, uint64_t *ref_size, void *stream);
+int lscomp_decompress_host_u16(lscomp_workspace *ws, const uint8_t *h_in, uint64_t cmp_len, uint32_t x, uint32_t y,
+                               uint32_t z, const uint32_t bins[4], float pooling, uint16_t *h_out, void *stream);
+int lscomp_decompress_host_u32(lscomp_workspace *ws, const uint8_t *h_in, uint64_t cmp_len, uint32_t x, uint32_t y,
+                               uint32_t z, const uint32_t bins[4], float pooling, uint32_t *h_out, void *stream);
+/* Input bytes per chunk of the host-memory calls on this workspace (whole
+   frames, at least one; 0 restores the default of 128 MB). */
+int lscomp_workspace_set_host_chunk(lscomp_workspace *ws, uint64_t bytes);
+
 /* uint16 compression that allocates nothing (no counterpart in the
    reference).  For callers that cannot allocate device memory when they
    compress -- acquisition loops running inside a fixed, pre-reserved memory

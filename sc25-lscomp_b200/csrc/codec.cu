@@ -205,6 +205,7 @@ int lscomp_workspace_destroy(lscomp_workspace *ws)
     int prev = 0;
     cudaGetDevice(&prev);
     cudaSetDevice(ws->device);
+    pipe_destroy(ws);
     if (ws->state) cudaFree(ws->state);
     if (ws->ctl) cudaFree(ws->ctl);
     if (ws->h_ctl) cudaFreeHost(ws->h_ctl);

@@ -29,6 +29,8 @@ struct lscomp_workspace {
     uint32_t *d_tile_stack = nullptr;
     uint64_t tile_stack_cap = 0;
     bool no_tune = false;              // calls through this workspace never tune
+    void *pipe = nullptr;              // host-memory calls: copy streams, slot buffers (host_pipe.cu)
+    uint64_t host_chunk_bytes = 0;     // host-memory calls: input bytes per chunk (0: the default)
     std::mutex mu;
 };
 
@@ -278,6 +280,9 @@ inline int read_ctl(lscomp_workspace *ws, cudaStream_t st)
     if (e != cudaSuccess) return cuda_status(e);
     return dev_status(ws->h_ctl->error);
 }
+
+// Frees the workspace's host-memory pipeline state (host_pipe.cu).
+void pipe_destroy(lscomp_workspace *ws);
 
 // ---------------------------------------------------------------- tuner
 // Launch configuration of one call: encoder CTA shape (-1: the rule of

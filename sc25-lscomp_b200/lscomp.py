@@ -101,6 +101,7 @@ def load_library() -> ctypes.CDLL:
     lib.lscomp_workspace_destroy.argtypes = [vp]
     lib.lscomp_workspace_check.argtypes = [vp, vp]
     lib.lscomp_workspace_set_tuning.argtypes = [vp, ctypes.c_int]
+    lib.lscomp_workspace_set_host_chunk.argtypes = [vp, u64]
     lib.lscomp_compress_u16.argtypes = [vp, vp, u32, u32, u32, bins_t, f32, vp, u64, pu64, pu64, vp]
     lib.lscomp_compress_u16_async.argtypes = [vp, vp, u32, u32, u32, bins_t, f32, vp, u64, vp, vp]
     lib.lscomp_decompress_u16.argtypes = [vp, vp, u64, u32, u32, u32, bins_t, f32, vp, vp]
@@ -140,6 +141,10 @@ def load_library() -> ctypes.CDLL:
                                                                  ctypes.POINTER(vp)]
     lib.lscomp_plan_run.argtypes = [vp, vp, pu64, pu64]
     lib.lscomp_plan_destroy.argtypes = [vp]
+    for sfx in ("u16", "u32"):
+        getattr(lib, f"lscomp_compress_host_{sfx}").argtypes = [vp, vp, u32, u32, u32, bins_t, f32, vp, u64, pu64,
+                                                               pu64, vp]
+        getattr(lib, f"lscomp_decompress_host_{sfx}").argtypes = [vp, vp, u64, u32, u32, u32, bins_t, f32, vp, vp]
     lib.lscomp_tune_mode.argtypes = [ctypes.c_int]
     lib.lscomp_tune_hits.restype = u64
     lib.lscomp_tune_report.restype = u64
@@ -187,6 +192,11 @@ class Workspace:
     @property
     def handle(self):
         return self._ws
+
+    def set_host_chunk(self, nbytes: int) -> None:
+        """Input bytes per chunk of compress_host / decompress_host (0: default)."""
+        _check(load_library().lscomp_workspace_set_host_chunk(self._ws, ctypes.c_uint64(int(nbytes))),
+               "lscomp_workspace_set_host_chunk")
 
     def set_tuning(self, allow: bool) -> None:
         """False: calls through this workspace never run the tuner."""
@@ -280,6 +290,54 @@ def compress_batch_mixed(ws: Workspace, items, stream=None):
                                                          ctypes.c_void_p(_stream_handle(stream)))
     _check(st, f"lscomp_compress_batch_ex_{sfx}")
     return [(int(sl[i]), int(rs[i])) for i in range(n)]
+
+
+def _host_buffer(a):
+    """(address, bytes, element bytes) of a host buffer: a numpy array or a
+    CPU torch tensor (pinned ones let the copies overlap)."""
+    if isinstance(a, np.ndarray):
+        if not a.flags["C_CONTIGUOUS"]:
+            raise ValueError("host buffer must be contiguous")
+        return a.ctypes.data, a.nbytes, a.itemsize
+    if getattr(a, "is_cuda", False):
+        raise ValueError("expected a host buffer")
+    return a.data_ptr(), a.numel() * a.element_size(), a.element_size()
+
+
+def compress_host(ws: Workspace, h_in, dims, bins, pooling: float, h_out, stream=None) -> Tuple[int, int]:
+    """Compress a stack in host memory (uint16 / uint32 values, or int16 /
+    int32 carrying them) into host buffer h_out (bytes).  Returns
+    (stream_len, ref_size), as compress_into."""
+    lib = load_library()
+    pi, ni, es = _host_buffer(h_in)
+    po, no, _ = _host_buffer(h_out)
+    x, y, z = (int(v) for v in dims)
+    if ni < x * y * z * es:
+        raise ValueError("input smaller than the dims")
+    sfx = "u32" if es == 4 else "u16"
+    sl, rs = ctypes.c_uint64(0), ctypes.c_uint64(0)
+    _check(getattr(lib, f"lscomp_compress_host_{sfx}")(ws.handle, ctypes.c_void_p(pi), x, y, z, _bins(bins),
+                                                       ctypes.c_float(pooling), ctypes.c_void_p(po),
+                                                       ctypes.c_uint64(no), ctypes.byref(sl), ctypes.byref(rs),
+                                                       ctypes.c_void_p(_stream_handle(stream))),
+           f"lscomp_compress_host_{sfx}")
+    return int(sl.value), int(rs.value)
+
+
+def decompress_host(ws: Workspace, h_cmp, cmp_len: int, dims, bins, pooling: float, h_out, stream=None) -> None:
+    """Decompress a stream in host memory (cmp_len readable bytes) into the
+    host buffer h_out (X*Y*Z values of 2 or 4 bytes)."""
+    lib = load_library()
+    pi, ni, _ = _host_buffer(h_cmp)
+    po, no, es = _host_buffer(h_out)
+    x, y, z = (int(v) for v in dims)
+    if no < x * y * z * es or ni < cmp_len:
+        raise ValueError("buffer smaller than the dims or the stream")
+    sfx = "u32" if es == 4 else "u16"
+    _check(getattr(lib, f"lscomp_decompress_host_{sfx}")(ws.handle, ctypes.c_void_p(pi), ctypes.c_uint64(int(cmp_len)),
+                                                         x, y, z, _bins(bins), ctypes.c_float(pooling),
+                                                         ctypes.c_void_p(po), ctypes.c_void_p(_stream_handle(stream))),
+           f"lscomp_decompress_host_{sfx}")
 
 
 def compress_batch(ws: Workspace, items, bins, pooling: float, stream=None):
