@@ -57,6 +57,9 @@ def parse():
     ap.add_argument("--serve", type=float, default=0.0,
                     help="serving benchmark: Poisson arrivals at this many requests per second (its own JSON line)")
     ap.add_argument("--serve-seconds", type=float, default=10.0)
+    ap.add_argument("--serve-max-mb", type=int, default=512, help="largest request of the serving benchmark")
+    ap.add_argument("--serve-arena-gb", type=int, default=32,
+                    help="device arena (and pinned staging) of the serving benchmark's server")
     ap.add_argument("--batch-frames", type=int, default=16, help="largest frame count of a batch stack")
     ap.add_argument("--ref-cpu", action="store_true",
                     help="with --impl reference: the oracle on the host cores instead of the reference's CUDA build")
@@ -413,15 +416,17 @@ def tuned_summary(lscomp, kinds=("compress", "batch", "decompress")):
 
 def bench_serve(args, local):
     """Serving loop under Poisson arrivals: requests of log-uniform size
-    (256 KB .. 64 MB of 1024x1024 or 1813x1558 uint16 frames), 70% compress /
-    30% decompress, 60% lossless / 40% lossy (-b 3 5 10 15 -p 0.5), host
-    buffers in and out.  Latency = queue + service time per request."""
+    (256 KB .. --serve-max-mb of 1024x1024 or 1813x1558 uint16 frames), 70%
+    compress / 30% decompress, 60% lossless / 40% lossy (-b 3 5 10 15
+    -p 0.5), host buffers in and out.  Latency = queue + service time per
+    request."""
     import lscomp
 
     rng = np.random.default_rng(5)
     pool = []
-    for i in range(24):
-        size = float(np.exp(rng.uniform(np.log(256 << 10), np.log(64 << 20))))
+    max_bytes = int(args.serve_max_mb) << 20
+    for i in range(32):
+        size = float(np.exp(rng.uniform(np.log(256 << 10), np.log(max_bytes))))
         h, w = (1024, 1024) if i % 2 else (1813, 1558)
         frames = max(1, int(round(size / (2 * h * w))))
         if size < 2 * h * w:
@@ -430,7 +435,7 @@ def bench_serve(args, local):
         kind = "xpcs" if i % 2 else "cssi"
         pool.append((dims, getattr(lscomp, f"synth_{kind}")(dims, seed=100 + i).reshape(dims)))
     modes = [("lossless", (1, 1, 1, 1), 1.0), ("lossy", (3, 5, 10, 15), 0.5)]
-    arena = 8 << 30
+    arena = int(args.serve_arena_gb) << 30
     srv = lscomp.Server(local, arena_bytes=arena)
     # containers of every pool stack in both modes, for the decompress requests
     conts = {}
@@ -494,9 +499,9 @@ def bench_serve(args, local):
                       "offered_req_per_s": rate, "achieved_req_per_s": round(n_sub / elapsed, 1),
                       "input_gb_per_s": round(nbytes_done[0] / elapsed / 1e9, 2),
                       "rounds": st["rounds"], "batches": st["batches"], "batched_requests": st["batched_requests"],
-                      "config": {"workload": "24 seeded stacks, log-uniform 256 KB..64 MB, 1024x1024 (XPCS-like) or "
-                                             "1813x1558 (CSSI-like) uint16 frames; 70/30 compress/decompress; "
-                                             "60/40 lossless/lossy", "arena_bytes": arena,
+                      "config": {"workload": f"32 seeded stacks, log-uniform 256 KB..{args.serve_max_mb} MB, "
+                                             "1024x1024 (XPCS-like) or 1813x1558 (CSSI-like) uint16 frames; 70/30 "
+                                             "compress/decompress; 60/40 lossless/lossy", "arena_bytes": arena,
                                  "duration_s": dur}}))
 
 
@@ -587,6 +592,8 @@ def main():
         td = float(np.mean([e[4 * i + 1].elapsed_time(e[4 * i + 2]) for e in evs]))
         sl = sizes[name]
         per[name] = {"compress_gbs": round(nbytes / tc / 1e6, 1), "decompress_gbs": round(nbytes / td / 1e6, 1),
+                     "compress_mib_per_ms": round(nbytes / 2**20 / tc, 1),
+                     "decompress_mib_per_ms": round(nbytes / 2**20 / td, 1),
                      "compress_ms": round(tc, 4), "decompress_ms": round(td, 4), "stream_bytes": sl,
                      "ratio": round(nbytes / sizes[name + "_ref_size"], 4),
                      "compress_hbm_frac": round((nbytes + sl) / tc / 1e6 / hbm, 4),
