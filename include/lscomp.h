@@ -218,8 +218,8 @@ int lscomp_plan_run(lscomp_plan *plan, void *stream, uint64_t *stream_len, uint6
 int lscomp_plan_destroy(lscomp_plan *plan);
 
 /* Launch-configuration tuner (no counterpart in the reference, whose launch
-   shape is fixed).  A configuration is the encoder CTA shape (2 groups of 8
-   or of 7 compute warps) and the most 8x8 blocks a tile holds (uint16: 256
+   shape is fixed).  A configuration is the encoder CTA shape (2 groups of 8,
+   7 or -- single stacks -- 13 compute warps) and the most 8x8 blocks a tile holds (uint16: 256
    or 128; uint32: 128 or 64); the decoder only has the tile size.  Every
    configuration writes the same stream.  With tuning on (the default;
    environment LSCOMP_AUTOTUNE=0 or lscomp_tune_mode(0) turns it off) the
@@ -236,7 +236,7 @@ int lscomp_plan_destroy(lscomp_plan *plan);
    previous mode.  lscomp_tune_report writes the table as text (one line per
    key: "es layout pool kind vec bzb -> shape tile_blocks", then
    " | shape tile_blocks ms" per timed candidate; kind 0 compress, 1 batch,
-   2 decompress; shape -1 = rule, 0 = 2x8, 1 = 2x7) and returns the bytes
+   2 decompress; shape -1 = rule, 0 = 2x8, 1 = 2x7, 2 = 2x13) and returns the bytes
    needed including the terminating NUL.  lscomp_tune_save / _load write and
    read that text (load replaces the keys it names; a malformed file changes
    nothing and returns LSCOMP_ERR_ARG).  Single stacks of fewer than 4

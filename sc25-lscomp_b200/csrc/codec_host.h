@@ -208,19 +208,30 @@ inline double unit_fill(const Geom &g, uint32_t wpg)
 
 // Shape of the encoder CTA when no tuned choice is known (shape < 0): the
 // lossless uint16 kernel is bound by its producer and writer warps and keeps
-// LSC_ENC_GROUPS x LSC_ENC_WPG; the lossy one is bound by its compute warps,
-// and when groups of 7 warps fill a tile's unit slots clearly better than
-// groups of 8 (a block-row of 195 blocks: 25 units, 89% against 78%) it runs
-// with 7 (measured on B200: CSSI-like lossy compress 2.71 -> 2.59 ms;
-// XPCS-like tiles of 32 units keep 8).  shape 0 / 1 force 2 x 8 / 2 x 7
-// (uint16 only; uint32 always runs 2 x 8).
+// LSC_ENC_GROUPS x LSC_ENC_WPG; the lossy one is bound by its compute warps
+// and takes, of groups of 8, 7 or 13 warps (a group's warps take a tile's
+// 8-block units round by round), the one that fills the unit slots best,
+// preferring 8 unless another is clearly better (a block-row of 195 blocks:
+// 25 units, 78% / 89% / 96%; measured on B200, CSSI-like lossy compress
+// 2.71 -> 2.59 ms with 7, 2.51 -> 2.37 ms with 13; XPCS-like tiles of 32
+// units keep 8).  Groups of 13 keep only the header bytes between the two
+// passes and read the rows again from the input slot (72 registers a
+// thread, 28 compute warps on the SM).  shape 0 / 1 / 2 force 2 x 8 / 2 x 7
+// / 2 x 13 (uint16; 2 x 13 for single stacks only; uint32 always runs 2 x 8).
+constexpr int kWideWpg = 13;
+
 template <typename T, int VEC, int BINS, bool POOL, bool BATCH>
 inline int launch_enc_t(const EncArgs<T> &a, int shape, int sm_count, cudaStream_t st)
 {
     if constexpr (sizeof(T) == 2 && LSC_ENC_GROUPS == 2 && LSC_ENC_WPG == 8) {
-        const bool seven = shape == 1 || (shape < 0 && BINS != BINS_IDENT && !BATCH &&
-                                          unit_fill(a.g, 7) > unit_fill(a.g, 8) + 0.05);
-        if (seven) return launch_enc_w<T, VEC, BINS, POOL, 2, 7, BATCH>(a, sm_count, st);
+        if (shape < 0 && BINS != BINS_IDENT && !BATCH) {
+            const double f8 = unit_fill(a.g, 8), f7 = unit_fill(a.g, 7), f13 = unit_fill(a.g, kWideWpg);
+            if (f13 > f8 + 0.05 && f13 >= f7) shape = 2;
+            else if (f7 > f8 + 0.05) shape = 1;
+        }
+        if constexpr (!BATCH)
+            if (shape == 2) return launch_enc_w<T, VEC, BINS, POOL, 2, kWideWpg, BATCH>(a, sm_count, st);
+        if (shape == 1) return launch_enc_w<T, VEC, BINS, POOL, 2, 7, BATCH>(a, sm_count, st);
     }
     return launch_enc_w<T, VEC, BINS, POOL, LSC_ENC_GROUPS, LSC_ENC_WPG, BATCH>(a, sm_count, st);
 }

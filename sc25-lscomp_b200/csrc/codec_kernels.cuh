@@ -1059,6 +1059,12 @@ template <typename T, int VEC, int BINS, bool POOL, int GRP, int WPG, bool BATCH
 __device__ __forceinline__ void enc_compute(const EncArgs<T> &a, EncSmem &sm)
 {
     constexpr int UMAX = (Elem<T>::kTileBlocks / 8 + WPG - 1) / WPG;  // units per warp per tile
+    // groups of more than 8 warps keep only the header bytes between the
+    // passes and read the rows again from the input slot in pass B (the slot
+    // is then released after pass B): fewer registers per thread, so more
+    // warps fit on the SM
+    constexpr bool RELOAD = WPG > 8;
+    constexpr int UKEEP = RELOAD ? 1 : UMAX;
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t grp = warp / WPG, wg = warp % WPG, gtid = tid - grp * WPG * 32;
     const uint32_t barid = kComputeBarrier + grp;
@@ -1080,9 +1086,9 @@ __device__ __forceinline__ void enc_compute(const EncArgs<T> &a, EncSmem &sm)
             }
             break;
         }
-        // the slot's batch fields are read before the slot is released after
-        // pass A (the producer may refill it while this tile is packed);
-        // g is only used in pass A
+        // the slot's batch fields are read before the slot is released (the
+        // producer may refill it while this tile is packed); g is only used
+        // while the slot is held
         const Geom &g = BATCH ? sm.in_geom[i] : a.g;
         uint8_t *const out = BATCH ? sm.in_out[i] : a.out;
         const BatchStack *const bstack = BATCH ? sm.in_stack[i] : nullptr;
@@ -1100,7 +1106,7 @@ __device__ __forceinline__ void enc_compute(const EncArgs<T> &a, EncSmem &sm)
 
         // ---- pass A: rows to registers, header bytes
         const uint32_t nunits = (ti.nblk + 7) >> 3;
-        Row<T> A[UMAX], B[UMAX];
+        Row<T> A[UKEEP], B[UKEEP];
         uint32_t hq[UMAX];
         uint32_t bad = 0;
 #pragma unroll
@@ -1111,9 +1117,14 @@ __device__ __forceinline__ void enc_compute(const EncArgs<T> &a, EncSmem &sm)
                 const uint32_t b = u * 8 + jb;
                 const bool active = b < ti.nblk;
                 SegLoc L = seg_locate<T, true>(g, ti, sm.br_rel[i], sm.br_rows[i], stage, sm.in_mis[i], active ? b : 0, r);
-                load_rows<T, VEC>(L, active, r, A[q], B[q]);
+                Row<T> ra, rb_;
+                load_rows<T, VEC>(L, active, r, ra, rb_);
+                if (!RELOAD) {
+                    A[RELOAD ? 0 : q] = ra;
+                    B[RELOAD ? 0 : q] = rb_;
+                }
                 uint32_t rb;
-                hq[q] = block_header<T, BINS == BINS_IDENT ? BINS_EQUAL : BINS, POOL, BINS == BINS_IDENT>(A[q], B[q], cA, rb);
+                hq[q] = block_header<T, BINS == BINS_IDENT ? BINS_EQUAL : BINS, POOL, BINS == BINS_IDENT>(ra, rb_, cA, rb);
                 if (active && r == 0) {
                     hdr[b] = (uint8_t)hq[q];
                     bad |= rb;
@@ -1121,7 +1132,7 @@ __device__ __forceinline__ void enc_compute(const EncArgs<T> &a, EncSmem &sm)
             }
         }
         __syncwarp();
-        if (lane == 0) mbar_arrive(&sm.in_empty[i]);  // the input slot may be refilled
+        if (!RELOAD && lane == 0) mbar_arrive(&sm.in_empty[i]);  // the input slot may be refilled
         if (!group_bar_and(barid, WPG * 32, bad == 0)) {
             // a uint32 quotient >= 2^31 needs 32 planes, which the 5-bit rate
             // field cannot hold
@@ -1150,9 +1161,21 @@ __device__ __forceinline__ void enc_compute(const EncArgs<T> &a, EncSmem &sm)
             if (u < nunits) {
                 const uint32_t b = u * 8 + jb;
                 const bool active = b < ti.nblk;
-                block_pack<T, BINS == BINS_IDENT>(A[q], B[q], hq[q], active, r, xs, cB,
-                                                   st + (active ? off[b] : 0u));
+                Row<T> ra, rb_;
+                if (RELOAD) {
+                    SegLoc L = seg_locate<T, true>(g, ti, sm.br_rel[i], sm.br_rows[i], stage, sm.in_mis[i],
+                                                   active ? b : 0, r);
+                    load_rows<T, VEC>(L, active, r, ra, rb_);
+                } else {
+                    ra = A[RELOAD ? 0 : q];
+                    rb_ = B[RELOAD ? 0 : q];
+                }
+                block_pack<T, BINS == BINS_IDENT>(ra, rb_, hq[q], active, r, xs, cB, st + (active ? off[b] : 0u));
             }
+        }
+        if (RELOAD) {
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&sm.in_empty[i]);  // the input slot may be refilled
         }
         // each warp reports its part of the packed tile; the writer waits for all
         if (gtid == 0) {

@@ -119,7 +119,7 @@ def force(lz, tmp_path, line):
     lz.tune_load(str(f))
 
 
-CANDIDATES = {2: [(0, 256), (1, 256), (0, 128), (1, 128)], 4: [(0, 128), (0, 64)]}
+CANDIDATES = {2: [(0, 256), (1, 256), (2, 256), (0, 128), (1, 128)], 4: [(0, 128), (0, 64)]}
 DEC_CANDIDATES = {2: [(-1, 256), (-1, 128)], 4: [(-1, 128), (-1, 64)]}
 SHAPES = [(3, 37, 53), (2, 17, 2100), (4, 64, 1024), (2, 40, 1558), (1, 9, 2049)]
 
