@@ -36,15 +36,11 @@
 #include "device_prims.cuh"
 
 // Tuning switches (compile-time; the defaults are the measured best on B200):
-//   LSC_WRITERS       writer warps per encoder CTA (1 or 2)
 //   LSC_LOOKBACK      0: 32-wide look-back to the nearest inclusive prefix,
 //                     1: 256-wide look-back bounded by the writer's previous tile
 //   LSC_DEC_CTAS      decoder CTAs per SM the register budget is sized for
 //   LSC_ENC_GROUPS    compute groups per encoder CTA (tiles in flight)
 //   LSC_ENC_WPG       warps per compute group
-#ifndef LSC_WRITERS
-#define LSC_WRITERS 1
-#endif
 #ifndef LSC_LOOKBACK
 #define LSC_LOOKBACK 0
 #endif
@@ -607,7 +603,7 @@ __device__ __forceinline__ uint32_t xpose4(uint32_t x, const XSel &s)
 // Encoder CTA: GRP x WPG compute warps in independent groups, one producer
 // warp (tile claims and TMA loads) and kWriters writer warps (look-back and
 // write-out, alternate tiles), one CTA per SM.
-constexpr int kWriters = LSC_WRITERS;         // writer warps, taking alternate tiles
+constexpr int kWriters = 1;                   // writer warps (look-back and write-out)
 template <int GRP, int WPG> struct EncShape {
     static constexpr int kCompute = GRP * WPG;
     static constexpr int kThreads = (kCompute + 1 + kWriters) * 32;
