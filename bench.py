@@ -220,7 +220,11 @@ def cpu_baseline(kind, dims, budget_s):
                       f"{t:.1f} s"}
 
 
-def dist_init(n):
+def dist_init(n, backend=None):
+    """One process per GPU under torchrun: NCCL for the barrier and the
+    max-over-ranks timing (gloo when no GPU is visible, as in the CPU tests
+    of this plumbing).  A short process-group timeout ends a rank that waits
+    for a dead peer with an error."""
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -230,8 +234,11 @@ def dist_init(n):
         import torch
         import torch.distributed as dist
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        if backend is None:
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return rank, world, local
 
 
@@ -241,7 +248,8 @@ def max_over_ranks(v, world):
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
