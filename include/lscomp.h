@@ -189,6 +189,18 @@ int lscomp_compress_batch_ex_u32(lscomp_workspace *ws, const lscomp_stack *stack
                                  const uint32_t *bins, const float *pooling, uint64_t *stream_len,
                                  uint64_t *ref_size, void *stream);
 
+/* Batch decompression (no counterpart in the reference): n streams decoded
+   by two launches (stream offsets for every stack, then one CTA per tile of
+   every stack).  stacks[i].d_in = the stream (4-byte aligned), .cap = its
+   readable bytes (at least the header), .d_out = X*Y*Z values of the call's
+   type, bins[4 i .. 4 i + 3] and pooling[i] its settings.  Every output
+   equals lscomp_decompress_u16 / _u32 of that stream alone.  Synchronises
+   the stream. */
+int lscomp_decompress_batch_u16(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, const uint32_t *bins,
+                                const float *pooling, void *stream);
+int lscomp_decompress_batch_u32(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, const uint32_t *bins,
+                                const float *pooling, void *stream);
+
 /* Graph plans (no counterpart in the reference).  A plan fixes one
    compression -- n stacks (n = 1: the single-stack kernel, n > 1: the batch
    kernel), their buffers and shapes, bins and pooling threshold -- and

@@ -9,6 +9,7 @@
 // once, so no look-back walk crosses into the previous stack.  Each stack's
 // stream is exactly the one lscomp_compress_u16/_u32 writes for it alone.
 #include <string.h>
+#include <algorithm>
 #include <mutex>
 #include <vector>
 #include "codec_host.h"
@@ -205,6 +206,98 @@ int compress_batch_t(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t 
             if (ref_size) ref_size[s] = total_s + geom[s].nb;
         }
     }
+    if (prev != ws->device) cudaSetDevice(prev);
+    return r;
+}
+
+// ---------------------------------------------------------------- batch decompression
+// Many streams decoded by two launches: the offsets kernel over every
+// stack's segments, then one CTA per tile of every stack.  stacks[i]: d_in =
+// stream, cap = its readable bytes, d_out = the decoded values (X*Y*Z of the
+// call's type), bins[4 i ..] and pooling[i] its settings.
+template <typename T>
+int decompress_batch_t(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, const uint32_t *bins,
+                       const float *pooling, void *stream)
+{
+    if (!ws || (n && (!stacks || !bins || !pooling))) return LSCOMP_ERR_ARG;
+    if (n == 0) return LSCOMP_OK;
+    std::vector<Codec> codec;
+    int layout = 0;
+    bool pool = false;
+    if (!batch_codecs(bins, pooling, true, n, sizeof(T) == 4, codec, layout, pool)) return LSCOMP_ERR_ARG;
+    std::vector<Geom> geom;
+    std::vector<unsigned long long> tile0;
+    unsigned long long total = 0;
+    if (!batch_geoms(stacks, n, Elem<T>::kTileBlocks, geom, tile0, total)) return LSCOMP_ERR_ARG;
+    int vec = 16;
+    std::vector<unsigned long long> seg0(n + 1, 0);
+    for (uint32_t s = 0; s < n; s++) {
+        const lscomp_stack &q = stacks[s];
+        if (!q.d_in || !q.d_out) return LSCOMP_ERR_ARG;
+        // the stream is read in 4-byte words, the values stored as T
+        if (reinterpret_cast<uintptr_t>(q.d_in) % 4u || reinterpret_cast<uintptr_t>(q.d_out) % sizeof(T))
+            return LSCOMP_ERR_ARG;
+        if (q.cap < geom[s].nb) return LSCOMP_ERR_CAPACITY;
+        const int v = vec_class(q.d_out, q.z, sizeof(T));
+        if (v < vec) vec = v;
+        seg0[s + 1] = seg0[s] + (geom[s].ntiles + kSegTiles - 1) / kSegTiles;
+    }
+    if (sizeof(T) == 4 && vec == 2) return LSCOMP_ERR_ARG;
+    if (total > 0x7fffffffull) return LSCOMP_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    std::lock_guard<std::mutex> lk(ws->mu);
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (prev != ws->device) cudaSetDevice(ws->device);
+    // look-back words: one per segment; tile offsets: ntiles + 1 per stack
+    const unsigned long long need = std::max<unsigned long long>(seg0[n], total + n);
+    int r = ws_prepare(ws, need, st);
+    if (!r) r = batch_reserve(ws, n, total, st);
+    if (!r) {
+        for (uint32_t s = 0; s < n; s++) {
+            BatchStack &b = ws->h_stacks[s];
+            b.g = geom[s];
+            b.c = codec[s];
+            b.in = stacks[s].d_in;
+            b.out = stacks[s].d_out;
+            b.cap = stacks[s].cap;
+            b.tile0 = tile0[s];
+            b.sizes = nullptr;
+        }
+        for (uint32_t s = 0; s <= n; s++) ws->h_bsizes[s] = seg0[s];  // pinned staging of the segment table
+        r = cuda_status(cudaMemcpyAsync(ws->d_stacks, ws->h_stacks, n * sizeof(BatchStack), cudaMemcpyHostToDevice, st));
+        if (!r)
+            r = cuda_status(cudaMemcpyAsync(ws->d_bsizes, ws->h_bsizes, (n + 1ull) * sizeof(unsigned long long),
+                                            cudaMemcpyHostToDevice, st));
+    }
+    if (!r) {
+        DecArgs<T> a;
+        memset(&a, 0, sizeof(a));
+        a.ctl = ws->ctl;
+        a.state = ws->state;
+        a.tile_off = ws->state + ws->state_cap;
+        a.epoch = ws->epoch;
+        a.stacks = ws->d_stacks;
+        a.nstacks = n;
+        a.seg0 = ws->d_bsizes;
+        unsigned long long grid = (unsigned long long)ws->sm_count * 4;
+        if (grid > seg0[n]) grid = seg0[n];
+        dec_offsets_batch_kernel<T><<<(unsigned)grid, kThreads, 0, st>>>(a);
+        g_launches.fetch_add(1);
+        r = cuda_status(cudaGetLastError());
+        if (!r) {
+            switch (vec) {
+            case 16: dec_kernel<T, 16, true><<<(unsigned)total, kThreads, 0, st>>>(a); break;
+            case 4: dec_kernel<T, 4, true><<<(unsigned)total, kThreads, 0, st>>>(a); break;
+            default:
+                if constexpr (sizeof(T) == 2) dec_kernel<T, 2, true><<<(unsigned)total, kThreads, 0, st>>>(a);
+                break;
+            }
+            g_launches.fetch_add(1);
+            r = cuda_status(cudaGetLastError());
+        }
+    }
+    if (!r) r = read_ctl(ws, st);  // synchronises the stream
     if (prev != ws->device) cudaSetDevice(prev);
     return r;
 }
@@ -442,6 +535,18 @@ int lscomp_compress_batch_ex_u32(lscomp_workspace *ws, const lscomp_stack *stack
                                  const float *pooling, uint64_t *stream_len, uint64_t *ref_size, void *stream)
 {
     return compress_batch_t<uint32_t>(ws, stacks, n, bins, pooling, true, stream_len, ref_size, stream);
+}
+
+int lscomp_decompress_batch_u16(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, const uint32_t *bins,
+                                const float *pooling, void *stream)
+{
+    return decompress_batch_t<uint16_t>(ws, stacks, n, bins, pooling, stream);
+}
+
+int lscomp_decompress_batch_u32(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, const uint32_t *bins,
+                                const float *pooling, void *stream)
+{
+    return decompress_batch_t<uint32_t>(ws, stacks, n, bins, pooling, stream);
 }
 
 int lscomp_plan_create_u16(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, const uint32_t bins[4],

@@ -278,7 +278,7 @@ inline int launch_dec_t(const DecArgs<T> &a, int sm_count, cudaStream_t st)
     if (e != cudaSuccess) return cuda_status(e);
     // 2) every tile independently
     if (a.g.ntiles > 0x7fffffffull) return LSCOMP_ERR_ARG;
-    dec_kernel<T, VEC><<<(unsigned)a.g.ntiles, kThreads, 0, st>>>(a);
+    dec_kernel<T, VEC, false><<<(unsigned)a.g.ntiles, kThreads, 0, st>>>(a);
     g_launches.fetch_add(1);
     return cuda_status(cudaGetLastError());
 }

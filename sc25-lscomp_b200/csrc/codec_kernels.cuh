@@ -157,6 +157,13 @@ struct DecArgs {
     unsigned long long *state;    // look-back state of the offsets kernel (per segment)
     unsigned long long *tile_off; // per-tile payload offsets
     uint32_t epoch;
+    // batch launches: the stacks (in = stream, out = decoded values, cap =
+    // readable stream bytes, tile0 = first tile over the batch), their
+    // count and the first segment of each (nstacks + 1 entries); stack s's
+    // tile offsets are tile_off[tile0 + s ...] (ntiles + 1 of them)
+    const struct BatchStack *stacks;
+    uint32_t nstacks;
+    const unsigned long long *seg0;
 };
 
 // ---------------------------------------------------------------- geometry
@@ -1424,6 +1431,77 @@ __global__ void __launch_bounds__(kThreads) dec_offsets_kernel(const DecArgs<T> 
     }
 }
 
+// Batch form of dec_offsets_kernel: segments numbered over all stacks (a
+// segment never spans two), each stack's first segment publishes its
+// inclusive prefix at once, so the look-back stays inside a stack.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) dec_offsets_batch_kernel(const DecArgs<T> a)
+{
+    __shared__ unsigned long long seg_s;
+    __shared__ uint32_t stk_s;
+    __shared__ uint32_t tsum[kSegTiles];
+    __shared__ uint32_t ok_s;
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const unsigned long long nseg = a.seg0[a.nstacks];
+    for (;;) {
+        if (tid == 0) {
+            const unsigned long long sg = aborted(a.ctl) ? nseg : atomicAdd(&a.ctl->ticket, 1ull);
+            seg_s = sg;
+            if (sg < nseg) {
+                // the last stack whose first segment is <= sg
+                uint32_t lo = 0, hi = a.nstacks - 1;
+                while (lo < hi) {
+                    const uint32_t mid = (lo + hi + 1) >> 1;
+                    if (a.seg0[mid] <= sg) lo = mid;
+                    else hi = mid - 1;
+                }
+                stk_s = lo;
+            }
+        }
+        __syncthreads();
+        const unsigned long long sg = seg_s;
+        if (sg >= nseg) break;
+        const uint32_t sk = stk_s;
+        const BatchStack &st = a.stacks[sk];
+        const Geom &g = st.g;
+        const uint8_t *in = static_cast<const uint8_t *>(st.in);
+        unsigned long long *tile_off = a.tile_off + st.tile0 + sk;
+        const unsigned long long ls = sg - a.seg0[sk];  // segment inside the stack
+        const unsigned long long t0 = ls * kSegTiles;
+        for (uint32_t q = warp; q < (uint32_t)kSegTiles; q += kWarps) {
+            const unsigned long long t = t0 + q;
+            uint32_t sum = 0;
+            if (t < g.ntiles) {
+                const TileInfo ti = tile_info(g, t);
+                for (uint32_t b = lane; b < ti.nblk; b += 32) {
+                    const uint32_t h = in[ti.k0 + b];
+                    sum += (h & 0x1fu) * ((h & 0x80u) ? 4u : 8u);
+                }
+            }
+            sum = __reduce_add_sync(0xffffffffu, sum);
+            if (lane == 0) tsum[q] = sum;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            const uint32_t v = tsum[lane];
+            uint32_t inc = v;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t x = __shfl_up_sync(0xffffffffu, inc, o);
+                if (lane >= (uint32_t)o) inc += x;
+            }
+            const uint32_t agg = __shfl_sync(0xffffffffu, inc, 31);
+            bool lok;
+            const unsigned long long base = tile_prefix(a.state + a.seg0[sk], ls, a.epoch, agg, a.ctl, lok);
+            if (lok && t0 + lane < g.ntiles) tile_off[t0 + lane] = base + (inc - v);
+            if (lok && t0 + lane == g.ntiles - 1) tile_off[g.ntiles] = base + inc;  // end of the payload
+            if (lane == 0) ok_s = lok ? 1u : 0u;
+        }
+        __syncthreads();
+        if (!ok_s) break;
+    }
+}
+
 // Plane words of one block for this lane (planes 8 grp + r and 8 grp + r + 4;
 // words 1 and 3 hold rows 4-7 of a plain block).  Loads only planes < rate.
 template <typename T>
@@ -1524,16 +1602,42 @@ __device__ __forceinline__ void dec_unit(const DecArgs<T> &a, const TileInfo &ti
 // meet in shared memory, and each block's offset is its in-warp offset plus
 // the totals of the warps before it (kept one per lane, read by shuffle).
 // Thread 0's bulk copy of the payload is in flight meanwhile.
-template <typename T, int VEC>
-__global__ void __launch_bounds__(kThreads, LSC_DEC_CTAS) dec_kernel(const DecArgs<T> a)
+template <typename T, int VEC, bool BATCH>
+__global__ void __launch_bounds__(kThreads, LSC_DEC_CTAS) dec_kernel(const DecArgs<T> a0)
 {
     constexpr int NG = Elem<T>::kGroups;
     static_assert(kThreads >= kMaxTileBlocks && kWarps <= 32, "one thread per block of a tile");
     __shared__ DecSmem sm;
-    const Geom &g = a.g;
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t jb = lane & 7, r = lane >> 3;
-    const unsigned long long t = blockIdx.x;
+    // batch launches: one CTA per tile of all stacks; thread 0 finds the
+    // tile's stack and puts that stack's arguments in shared memory
+    __shared__ DecArgs<T> sa;
+    __shared__ unsigned long long st_s;
+    if constexpr (BATCH) {
+        if (tid == 0) {
+            const unsigned long long tg = blockIdx.x;
+            uint32_t lo = 0, hi = a0.nstacks - 1;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi + 1) >> 1;
+                if (a0.stacks[mid].tile0 <= tg) lo = mid;
+                else hi = mid - 1;
+            }
+            const BatchStack &bs = a0.stacks[lo];
+            sa = a0;
+            sa.g = bs.g;
+            sa.c = bs.c;
+            sa.in = static_cast<const uint8_t *>(bs.in);
+            sa.out = reinterpret_cast<T *>(bs.out);
+            sa.cap = bs.cap;
+            sa.tile_off = a0.tile_off + bs.tile0 + lo;
+            st_s = tg - bs.tile0;
+        }
+        __syncthreads();
+    }
+    const DecArgs<T> &a = BATCH ? sa : a0;
+    const Geom &g = a.g;
+    const unsigned long long t = BATCH ? st_s : (unsigned long long)blockIdx.x;
     if (t >= g.ntiles) return;
     const unsigned long long base = a.tile_off[t], end = a.tile_off[t + 1];
 

@@ -136,6 +136,8 @@ def load_library() -> ctypes.CDLL:
         getattr(lib, f"lscomp_compress_batch_ex_{sfx}").argtypes = [vp, ctypes.POINTER(LscompStack), u32,
                                                                     ctypes.POINTER(u32), ctypes.POINTER(f32),
                                                                     pu64, pu64, vp]
+        getattr(lib, f"lscomp_decompress_batch_{sfx}").argtypes = [vp, ctypes.POINTER(LscompStack), u32,
+                                                                   ctypes.POINTER(u32), ctypes.POINTER(f32), vp]
         getattr(lib, f"lscomp_plan_create_ex_{sfx}").argtypes = [vp, ctypes.POINTER(LscompStack), u32,
                                                                  ctypes.POINTER(u32), ctypes.POINTER(f32), vp,
                                                                  ctypes.POINTER(vp)]
@@ -338,6 +340,27 @@ def decompress_host(ws: Workspace, h_cmp, cmp_len: int, dims, bins, pooling: flo
                                                          x, y, z, _bins(bins), ctypes.c_float(pooling),
                                                          ctypes.c_void_p(po), ctypes.c_void_p(_stream_handle(stream))),
            f"lscomp_decompress_host_{sfx}")
+
+
+def decompress_batch(ws: Workspace, items, stream=None) -> None:
+    """Decode many streams in two launches: items = [(d_stream, cmp_len, dims,
+    d_out, bins, pooling), ...], d_out int16 (uint16 data) or int32 (uint32)
+    tensors of one type."""
+    lib = load_library()
+    n = len(items)
+    if n == 0:
+        return
+    sfx = _suffix(items[0][3])
+    arr = (LscompStack * n)()
+    for i, (d_s, ln, dims, d_out, b, p) in enumerate(items):
+        if _suffix(d_out) != sfx:
+            raise ValueError("a batch holds one element type")
+        x, y, z = (int(v) for v in dims)
+        arr[i] = LscompStack(d_s.data_ptr(), x, y, z, d_out.data_ptr(), int(ln))
+    bins, pool = _per_stack_settings([(None, None, None, it[4], it[5]) for it in items])
+    _check(getattr(lib, f"lscomp_decompress_batch_{sfx}")(ws.handle, arr, n, bins, pool,
+                                                          ctypes.c_void_p(_stream_handle(stream))),
+           f"lscomp_decompress_batch_{sfx}")
 
 
 def compress_batch(ws: Workspace, items, bins, pooling: float, stream=None):

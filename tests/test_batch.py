@@ -220,3 +220,41 @@ def test_mixed_settings_plan(lz, ws):
                 assert np.array_equal(out[:sl].cpu().numpy(), ref), (rnd, dims)
     finally:
         plan.close()
+
+
+@pytest.mark.parametrize("wide", [False, True])
+def test_decompress_batch(lz, ws, wide):
+    # streams of many shapes and settings decoded in one batch; each output
+    # must equal the single-stream decode (every element written)
+    rng = np.random.default_rng(21)
+    shapes = SHAPES + [(3, 130, 150), (2, 300, 210), (40, 9, 9)]
+    es = 4 if wide else 2
+    items, refs = [], []
+    for i, dims in enumerate(shapes):
+        b, p = SETTINGS[int(rng.integers(0, len(SETTINGS)))]
+        a = stack32(dims, seed=700 + i) if wide else stack16(dims, seed=700 + i)
+        view = np.int32 if wide else np.int16
+        d_in = torch.from_numpy(a.view(view).ravel()).cuda()
+        out = torch.zeros(lz.max_stream_bytes(dims, es), dtype=torch.uint8, device="cuda")
+        sl, _ = lz.compress_into(ws, d_in, dims, b, p, out)
+        ref = torch.empty_like(d_in)
+        lz.decompress_into(ws, out, sl, dims, b, p, ref)
+        dec = torch.full_like(d_in, -1)  # poison: every element must be written
+        items.append((out, sl, dims, dec, b, p))
+        refs.append(ref)
+    lz.decompress_batch(ws, items)
+    for (out, sl, dims, dec, b, p), ref in zip(items, refs):
+        assert torch.equal(dec, ref), (dims, b, p)
+
+
+def test_decompress_batch_truncated(lz, ws):
+    dims = (2, 64, 64)
+    d_in = torch.from_numpy(stack16(dims, seed=3).view(np.int16).ravel()).cuda()
+    out = torch.zeros(lz.max_stream_bytes(dims), dtype=torch.uint8, device="cuda")
+    sl, _ = lz.compress_into(ws, d_in, dims, *LOSSLESS, out)
+    dec = torch.empty_like(d_in)
+    with pytest.raises(lz.LscompError):
+        lz.decompress_batch(ws, [(out, sl - 16, dims, dec, *LOSSLESS), (out, sl, dims, torch.empty_like(d_in), *LOSSLESS)])
+    # the workspace still works
+    lz.decompress_batch(ws, [(out, sl, dims, dec, *LOSSLESS)])
+    assert torch.equal(dec, d_in)
