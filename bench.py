@@ -393,7 +393,26 @@ def bench_batch(args, local):
                 lscomp.compress_into(ws, d_in[f * fsz:(f + 1) * fsz], (1, dims[1], dims[2]), bins, p, scratch)
 
     t_frame = timed(loop_frame, max(1, args.steps // 2))
+    # decode every stream back: one batch-decompression call against one
+    # plain call per stack (outputs in a third buffer; checked against the
+    # inputs for the lossless stacks)
+    d_dec_all = torch.empty_like(d_in_all)
+    ditems = [(d_out, sl, dims, d_dec_all[oi:oi + (d_in.numel())], bins, p)
+              for (d_in, dims, d_out, bins, p), (sl, _), oi in zip(items, got, offs_in)]
+    lscomp.decompress_batch(ws, ditems)
+    for (d_in, dims, d_out, bins, p), dit in zip(items[::step], ditems[::step]):
+        if bins == (1, 1, 1, 1):
+            assert torch.equal(dit[3], d_in), "batch decode differs from the input (lossless)"
+    t_dbatch = timed(lambda: lscomp.decompress_batch(ws, ditems), args.steps)
+
+    def loop_dstack():
+        for d_s, sl, dims, d_o, bins, p in ditems:
+            lscomp.decompress_into(ws, d_s, sl, dims, bins, p, d_o)
+
+    t_dstack = timed(loop_dstack, args.steps)
     res = {"batch_call_ms": round(t_batch, 3), "graph_plan_ms": round(t_plan, 3),
+           "decompress_batch_call_ms": round(t_dbatch, 3), "decompress_per_stack_calls_ms": round(t_dstack, 3),
+           "decompress_frames_per_s": {"batch_call": fps(t_dbatch), "per_stack_calls": fps(t_dstack)},
            "per_stack_calls_ms": round(t_stack, 3), "per_frame_calls_ms": round(t_frame, 3),
            "frames_per_s": {"graph_plan": fps(t_plan), "batch_call": fps(t_batch), "per_stack_calls": fps(t_stack),
                             "per_frame_calls": fps(t_frame)},
