@@ -211,8 +211,9 @@ int compress_batch_t(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t 
 }
 
 // ---------------------------------------------------------------- batch decompression
-// Many streams decoded by two launches: the offsets kernel over every
-// stack's segments, then one CTA per tile of every stack.  stacks[i]: d_in =
+// Many streams decoded by three launches: the stack of every tile, the
+// offsets kernel over every stack's segments, then one CTA per tile of every
+// stack.  stacks[i]: d_in =
 // stream, cap = its readable bytes, d_out = the decoded values (X*Y*Z of the
 // call's type), bins[4 i ..] and pooling[i] its settings.
 template <typename T>
@@ -280,11 +281,18 @@ int decompress_batch_t(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_
         a.stacks = ws->d_stacks;
         a.nstacks = n;
         a.seg0 = ws->d_bsizes;
-        unsigned long long grid = (unsigned long long)ws->sm_count * 4;
-        if (grid > seg0[n]) grid = seg0[n];
-        dec_offsets_batch_kernel<T><<<(unsigned)grid, kThreads, 0, st>>>(a);
+        a.tile_stack = ws->d_tile_stack;
+        const uint32_t mgrid = n < 4096u ? n : 4096u;
+        tile_stack_kernel<<<mgrid, 256, 0, st>>>(ws->d_stacks, n, ws->d_tile_stack);
         g_launches.fetch_add(1);
         r = cuda_status(cudaGetLastError());
+        unsigned long long grid = (unsigned long long)ws->sm_count * 4;
+        if (grid > seg0[n]) grid = seg0[n];
+        if (!r) {
+            dec_offsets_batch_kernel<T><<<(unsigned)grid, kThreads, 0, st>>>(a);
+            g_launches.fetch_add(1);
+            r = cuda_status(cudaGetLastError());
+        }
         if (!r) {
             switch (vec) {
             case 16: dec_kernel<T, 16, true><<<(unsigned)total, kThreads, 0, st>>>(a); break;

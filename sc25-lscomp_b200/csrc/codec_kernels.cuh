@@ -164,6 +164,7 @@ struct DecArgs {
     const struct BatchStack *stacks;
     uint32_t nstacks;
     const unsigned long long *seg0;
+    const uint32_t *tile_stack;  // the stack of every tile over the batch
 };
 
 // ---------------------------------------------------------------- geometry
@@ -1610,19 +1611,14 @@ __global__ void __launch_bounds__(kThreads, LSC_DEC_CTAS) dec_kernel(const DecAr
     __shared__ DecSmem sm;
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t jb = lane & 7, r = lane >> 3;
-    // batch launches: one CTA per tile of all stacks; thread 0 finds the
+    // batch launches: one CTA per tile of all stacks; thread 0 looks up the
     // tile's stack and puts that stack's arguments in shared memory
     __shared__ DecArgs<T> sa;
     __shared__ unsigned long long st_s;
     if constexpr (BATCH) {
         if (tid == 0) {
             const unsigned long long tg = blockIdx.x;
-            uint32_t lo = 0, hi = a0.nstacks - 1;
-            while (lo < hi) {
-                const uint32_t mid = (lo + hi + 1) >> 1;
-                if (a0.stacks[mid].tile0 <= tg) lo = mid;
-                else hi = mid - 1;
-            }
+            const uint32_t lo = a0.tile_stack[tg];
             const BatchStack &bs = a0.stacks[lo];
             sa = a0;
             sa.g = bs.g;
