@@ -220,8 +220,11 @@ void run_round(lscomp_server *s, std::vector<Request *> &round)
                                                                 bins.data(), pool.data(), len.data(), ref.data(), s->st)
                                  : lscomp_compress_batch_ex_u32(s->ws, stacks.data(), (uint32_t)grp.size(),
                                                                 bins.data(), pool.data(), len.data(), ref.data(), s->st);
-        s->batches++;
-        s->batched_requests += grp.size();
+        {
+            std::lock_guard<std::mutex> lk(s->mu);  // lscomp_server_stats reads these under the lock
+            s->batches++;
+            s->batched_requests += grp.size();
+        }
         for (size_t g = 0; g < grp.size(); g++) {
             const size_t j = grp[g];
             Request *q = round[j];
