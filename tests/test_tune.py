@@ -50,11 +50,11 @@ def test_table_roundtrip(lzc, tmp_path):
     try:
         lzc.tune_clear()
         f = tmp_path / "t.txt"
-        f.write_text("# comment\n2 1 1 0 16 195 -> 1 256\n2 3 0 2 16 128 -> -1 128\n4 1 1 1 16 0 -> 0 64\n")
+        f.write_text("# comment\n2 1 1 0 16 195 -> 2 256\n2 3 0 2 16 128 -> -1 128\n4 1 1 1 16 0 -> 0 64\n")
         lzc.tune_load(str(f))
         tab = {(e["es"], e["layout"], e["pool"], e["kind"], e["vec"], e["bzb"]): (e["shape"], e["tile_blocks"])
                for e in lzc.tune_table()}
-        assert tab == {(2, 1, 1, "compress", 16, 195): (1, 256), (2, 3, 0, "decompress", 16, 128): (-1, 128),
+        assert tab == {(2, 1, 1, "compress", 16, 195): (2, 256), (2, 3, 0, "decompress", 16, 128): (-1, 128),
                        (4, 1, 1, "batch", 16, 0): (0, 64)}
         g = tmp_path / "g.txt"
         lzc.tune_save(str(g))
@@ -64,7 +64,10 @@ def test_table_roundtrip(lzc, tmp_path):
         assert len(lzc.tune_table()) == 3
         # malformed or out-of-range lines change nothing
         for bad in ("2 1 1 0 16 195 -> 1 300\n", "4 1 1 0 16 9 -> 1 128\n", "2 1 1 0 16\n", "2 9 1 0 16 1 -> 0 8\n",
-                    "4 1 1 0 2 9 -> 0 64\n", "2 1 1 0 8 9 -> 0 64\n"):
+                    "4 1 1 0 2 9 -> 0 64\n", "2 1 1 0 8 9 -> 0 64\n",
+                    "2 1 1 1 16 0 -> 2 256\n",   # 2 x 13 runs single stacks only
+                    "4 1 1 0 16 9 -> 2 128\n",   # and uint16 only
+                    "2 1 1 0 16 9 -> 3 256\n"):
             f.write_text("2 1 1 0 16 7 -> 0 8\n" + bad)
             with pytest.raises(lzc.LscompError):
                 lzc.tune_load(str(f))
