@@ -13,15 +13,18 @@
 //     so every tile a CTA waits on in the scan belongs to a resident CTA.
 //   * Encoder (one CTA per SM, warp-specialised): a producer warp fetches
 //     each tile's input once with 1-D TMA bulk copies into a 3-deep ring;
-//     16 compute warps take the rows into registers, derive every block's
-//     statistics, pooling, bin choice and rate, publish the tile's payload
-//     size and pack the bit planes into a 3-deep payload ring; a writer warp
-//     runs the decoupled look-back for the tile's stream offset and copies
-//     the packed payload to the stream.  Only the writer waits on other
-//     CTAs, and the compute warps run up to three tiles ahead of it.
+//     two groups of compute warps (8, 7 or 13 warps each, the shape chosen
+//     per call) take alternate tiles, derive every block's statistics,
+//     pooling, bin choice and rate, publish the tile's payload size and
+//     pack the bit planes into a 3-deep payload ring; a writer warp runs
+//     the decoupled look-back for the tile's stream offset and copies the
+//     packed payload to the stream.  Only the writer waits on other CTAs,
+//     and the compute warps run up to three tiles ahead of it.  Batch
+//     launches do the same over the tiles of many stacks.
 //   * Decoder: a small kernel turns the header bytes into per-tile stream
 //     offsets; the decode kernel then handles every tile independently
-//     (plane words gathered per block, values scattered to the rows).
+//     (plane words gathered per block, values scattered to the rows), for
+//     one stack or, in batch launches, for the tiles of many.
 //
 // Thread layout inside a warp ("unit" = 8 consecutive blocks of a tile):
 // lane = j + 8 r, j = block within the unit, r = 0..3; the lane owns rows r
