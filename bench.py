@@ -41,6 +41,21 @@ DIMS = (600, 1813, 1558)
 MODES = [("lossless", (1, 1, 1, 1), 1.0), ("lossy", (3, 5, 10, 15), 0.5)]
 SEED = 2
 FALLBACK_HBM_GBS = 6650.0
+L2_BYTES = 126 * 2**20
+KIND_NAMES = {"cssi": "CSSI-like", "xpcs": "XPCS-like", "small": "small (Poisson background, spots, hot pixels)"}
+# the benchmark set's other plain stacks, measured beside the headline one
+# (each mode: one compress and one decompress per repetition)
+PER_CONFIG = [("xpcs", (512, 1024, 1024)), ("small", (64, 256, 256))]
+
+
+def l2_note(nbytes):
+    if nbytes > L2_BYTES:
+        return f"inputs ({nbytes / 1e9:.2f} GB) larger than L2 (126 MB); no flush needed"
+    return f"inputs ({nbytes / 1e6:.1f} MB) fit in L2 (126 MB): a 256 MB buffer is written between timed passes"
+
+
+def data_note(kind):
+    return f"synthetic (seeded {KIND_NAMES[kind]} generator)"
 
 
 def parse():
@@ -53,6 +68,8 @@ def parse():
     ap.add_argument("--kind", default="cssi", choices=["cssi", "xpcs", "small"])
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-per-config", action="store_true",
+                    help="skip the XPCS-like and small stacks measured beside the default CSSI-like one")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--serve", type=float, default=0.0,
                     help="serving benchmark: Poisson arrivals at this many requests per second (its own JSON line)")
@@ -559,10 +576,10 @@ def main():
     cap = (lambda nb: (nb + 3) // 4 * 4 + 128 * nb)(dims[0] * ((dims[1] + 7) // 8) * ((dims[2] + 7) // 8))
     d_cmp = torch.zeros(cap, dtype=torch.uint8, device=dev)
     d_dec = torch.empty_like(d_in)
-    config = {"workload": f"{args.kind}-like stack {dims[0]}x{dims[1]}x{dims[2]} uint16, z fastest",
+    config = {"workload": f"{KIND_NAMES[args.kind]} stack {dims[0]}x{dims[1]}x{dims[2]} uint16, z fastest",
               "modes": "lossless -b 1 1 1 1 -p 1; lossy -b 3 5 10 15 -p 0.5",
               "step": "compress+decompress in both modes (4 passes)",
-              "input_bytes": nbytes, "l2": "inputs (3.39 GB) larger than L2 (126 MB); no flush needed",
+              "input_bytes": nbytes, "l2": l2_note(nbytes),
               "parallelism": f"replicas{world}"}
 
     if args.impl == "reference":
@@ -584,7 +601,9 @@ def main():
             if ev is not None:
                 ev[4 * i + 2].record(stream)
 
-    # exact stream lengths (and a correctness check) before timing
+    # exact stream lengths and a correctness check before timing; the
+    # device streams and decodes are kept on the host for the e2e check
+    expect = {}
     for name, bins, p in MODES:
         sl, rs = lscomp.compress_into(ws, d_in, dims, bins, p, d_cmp)
         sizes[name] = sl
@@ -592,6 +611,8 @@ def main():
         lscomp.decompress_into(ws, d_cmp, sl, dims, bins, p, d_dec)
         if name == "lossless" and not torch.equal(d_dec, d_in):
             raise SystemExit("lossless round trip failed")
+        if args.e2e_steps > 0:
+            expect[name] = (d_cmp[:sl].cpu(), d_dec.cpu())
     for _ in range(max(args.warmup, 3)):
         step()
     ws.check()
@@ -646,14 +667,21 @@ def main():
             pass
     value = world * 4 * nbytes / (ms_step / 1e3) / 1e9
 
-    e2e = bench_e2e(args, dims, ws, h, dev, nbytes, sizes, world) if args.e2e_steps > 0 else None
+    e2e = bench_e2e(args, dims, ws, h, dev, nbytes, sizes, world, expect) if args.e2e_steps > 0 else None
+    del expect
+    per_config = None
+    if not args.no_per_config and args.dims is None and args.kind == "cssi":
+        del d_cmp, d_dec
+        per_config = bench_per_config(args, lambda kind, pdims: codec_ours(ws, lscomp, pdims), local)
     out = {"metric": "lsCOMP compress+decompress throughput (lossless and lossy b=3 5 10 15 p=0.5), "
                      "uncompressed GB per second",
            "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
            "warmup": max(args.warmup, 3), "ms_per_step": round(ms_step, 4), "higher_is_better": True,
-           "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic (seeded CSSI-like generator)",
+           "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": data_note(args.kind),
            "config": config, "per_mode": per, "roofline": roofline, "e2e": e2e, "gpu_launches": int(launches),
            "clocks": clk, "tuned": tuned_summary(lscomp)}
+    if per_config is not None:
+        out["per_config"] = per_config
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args.kind, dims, args.cpu_seconds)
     if rank == 0:
@@ -664,13 +692,16 @@ def main():
         dist.destroy_process_group()
 
 
-def bench_e2e(args, dims, ws, h, dev, nbytes, sizes, world):
+def bench_e2e(args, dims, ws, h, dev, nbytes, sizes, world, expect):
     """Host buffers in, host buffers out, through the C ABI's host-memory
     calls (lscomp_compress_host_u16 / lscomp_decompress_host_u16): per mode
     the stack in pinned host memory is compressed into a host stream buffer,
     and that stream decompressed into a host stack buffer; every byte crosses
     PCIe inside the timed region (the calls pipeline chunks of frames so
-    copies up, kernels and copies down overlap)."""
+    copies up, kernels and copies down overlap).  Before timing, one pass per
+    mode is checked: its stream must equal the device-memory call's byte for
+    byte (expect[mode][0]) and its decode the device decode (expect[mode][1],
+    equal to the input for the lossless mode)."""
     import torch
 
     import lscomp
@@ -691,9 +722,18 @@ def bench_e2e(args, dims, ws, h, dev, nbytes, sizes, world):
             moved["d2h"] += sl + nbytes  # the stream down, then the stack down
         torch.cuda.synchronize()
 
+    for name, bins, p in MODES:
+        sl, _ = lscomp.compress_host(ws, h_in, dims, bins, p, h_cmp)
+        want_s, want_d = expect[name]
+        if sl != want_s.numel() or not torch.equal(h_cmp[:sl], want_s):
+            raise SystemExit(f"e2e ({name}): host-memory stream differs from the device-memory stream")
+        h_out.fill_(-1)
+        lscomp.decompress_host(ws, h_cmp, sl, dims, bins, p, h_out)
+        if not torch.equal(h_out, want_d):
+            raise SystemExit(f"e2e ({name}): host-memory decode differs from the device decode")
+        if name == "lossless" and not torch.equal(h_out, h_in):
+            raise SystemExit("e2e round trip failed (lossless decode differs from the input)")
     step()
-    if not torch.equal(h_out, h_in) and MODES[-1][0] == "lossless":
-        raise SystemExit("e2e round trip failed")
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier(world)
     torch.cuda.synchronize()
@@ -705,8 +745,94 @@ def bench_e2e(args, dims, ws, h, dev, nbytes, sizes, world):
     ms = max_over_ranks(e0.elapsed_time(e1), world) / args.e2e_steps
     return {"value": round(world * 4 * nbytes / (ms / 1e3) / 1e9, 2), "unit": "GB/s",
             "h2d_bytes_per_step": int(moved["h2d"]), "d2h_bytes_per_step": int(moved["d2h"]),
-            "ms_per_step": round(ms, 3),
+            "ms_per_step": round(ms, 3), "checked": "streams and decodes equal the device-memory calls' (both modes)",
             "path": "lscomp_compress_host_u16 / lscomp_decompress_host_u16 (C ABI), pinned host buffers"}
+
+
+def codec_ours(ws, lscomp, dims):
+    """(compress, decompress) callables of this library for bench_per_config."""
+
+    def comp(d_in, bins, p, d_cmp):
+        lscomp.compress_async(ws, d_in, dims, bins, p, d_cmp)
+
+    def decomp(d_cmp, sl, bins, p, d_dec):
+        lscomp.decompress_async(ws, d_cmp, sl, dims, bins, p, d_dec)
+
+    def sizes(d_in, bins, p, d_cmp):
+        return lscomp.compress_into(ws, d_in, dims, bins, p, d_cmp)
+
+    return comp, decomp, sizes
+
+
+def codec_ref(ref, dims):
+    """(compress, decompress) callables of the reference's host API."""
+
+    def comp(d_in, bins, p, d_cmp):
+        ref.compress(d_in.data_ptr(), d_cmp.data_ptr(), dims, bins, p)
+
+    def decomp(d_cmp, sl, bins, p, d_dec):
+        ref.decompress(d_dec.data_ptr(), d_cmp.data_ptr(), sl, dims, bins, p)
+
+    def sizes(d_in, bins, p, d_cmp):
+        d_cmp.zero_()
+        rs = ref.compress(d_in.data_ptr(), d_cmp.data_ptr(), dims, bins, p)
+        return rs, rs
+
+    return comp, decomp, sizes
+
+
+def bench_per_config(args, make_codec, local, reps=6):
+    """The other plain stacks of the benchmark set (XPCS-like 512x1024x1024,
+    small 64x256x256): per mode the median device time of one compress and
+    one decompress (CUDA events around each call, inputs resident in HBM),
+    GB/s of input and the fraction of the measured HBM copy bandwidth the
+    algorithmic bytes reach.  A stack that fits in L2 gets a 256 MB buffer
+    written before every timed call."""
+    import torch
+
+    hbm, _ = peaks()
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 * 2**20, dtype=torch.uint8, device=dev)
+    res = {}
+    for kind, dims in PER_CONFIG:
+        nbytes = 2 * dims[0] * dims[1] * dims[2]
+        d_in = torch.from_numpy(make_stack(kind, dims).view(np.int16)).to(dev)
+        nb = dims[0] * ((dims[1] + 7) // 8) * ((dims[2] + 7) // 8)
+        d_cmp = torch.zeros((nb + 3) // 4 * 4 + 128 * nb, dtype=torch.uint8, device=dev)
+        d_dec = torch.empty_like(d_in)
+        comp, decomp, sizes = make_codec(kind, dims)
+        small = nbytes <= L2_BYTES
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+        def timed(fn):
+            for _ in range(3):
+                fn()
+            ts = []
+            for _ in range(reps):
+                if small:
+                    flush.fill_(1)
+                e0.record(stream)
+                fn()
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ts.append(e0.elapsed_time(e1))
+            return float(np.median(ts))
+
+        per = {}
+        for name, bins, p in MODES:
+            sl, rs = sizes(d_in, bins, p, d_cmp)
+            tc = timed(lambda: comp(d_in, bins, p, d_cmp))
+            td = timed(lambda: decomp(d_cmp, sl, bins, p, d_dec))
+            per[name] = {"compress_ms": round(tc, 4), "decompress_ms": round(td, 4),
+                         "compress_gbs": round(nbytes / tc / 1e6, 1), "decompress_gbs": round(nbytes / td / 1e6, 1),
+                         "compress_hbm_frac": round((nbytes + sl) / tc / 1e6 / hbm, 4),
+                         "decompress_hbm_frac": round((nbytes + sl) / td / 1e6 / hbm, 4),
+                         "stream_bytes": int(sl), "ratio": round(nbytes / rs, 4)}
+        res[f"{KIND_NAMES[kind].split(' ')[0]} {dims[0]}x{dims[1]}x{dims[2]}"] = {
+            "modes": per, "input_bytes": nbytes, "l2": l2_note(nbytes), "data": data_note(kind)}
+        del d_in, d_cmp, d_dec
+    return res
 
 
 def bench_reference(args, dims, rank, world, dev, d_in, d_cmp, d_dec, nbytes, config, h):
@@ -752,7 +878,7 @@ def bench_reference_cpu(args, dims, config):
     x, y, z = dims
 
     def sample(nf):
-        return getattr(lscomp, "synth_cssi")(dims, seed=SEED, frames=(0, nf))
+        return getattr(lscomp, f"synth_{args.kind}")(dims, seed=SEED if args.kind == "cssi" else 1, frames=(0, nf))
 
     def step(a, nf):
         d = (nf, y, z)
@@ -773,14 +899,15 @@ def bench_reference_cpu(args, dims, config):
     sec = float(np.mean(ts))
     sbytes = a.size * 2
     value = 4 * sbytes / sec / 1e9
-    smp = (f"first {nf} of {x} frames ({sbytes / 1e9:.3f} GB) of the same CSSI-like stack per step, lossless + "
+    smp = (f"first {nf} of {x} frames ({sbytes / 1e9:.3f} GB) of the same {KIND_NAMES[args.kind]} stack per step, "
+           "lossless + "
            f"lossy compress + decompress, {sec:.2f} s per step")
     return {"impl": "reference",
             "metric": "lsCOMP compress+decompress throughput (lossless and lossy b=3 5 10 15 p=0.5), "
                       "uncompressed GB per second",
             "value": round(value, 3), "unit": "GB/s", "n_gpus": 1, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": round(sec * 1e3, 1), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic (seeded CSSI-like generator)",
+            "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": data_note(args.kind),
             "config": config,
             "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": threads, "kind": "port",
                              "sample": smp + "; the reference has no CPU implementation, so the oracle (its "
@@ -789,39 +916,62 @@ def bench_reference_cpu(args, dims, config):
 
 
 def bench_reference_gpu(args, dims, dev, d_in, d_cmp, d_dec, nbytes, config, h):
+    """Both builds of the reference's CUDA sources are timed on the same
+    steps -- nvcc -O3 for sm_100a, and nvcc's default target as the
+    reference's own CMake builds it (PTX compiled by the driver on B200) --
+    and the faster one is the arm's value, e2e and per-config figures."""
     import torch
 
     try:
-        from oracle import REF_LIB, RefLib
+        from oracle import REF_LIB, REF_LIB_DEFAULT, RefLib
 
-        ref = RefLib(REF_LIB)
+        refs = [("sm_100a", RefLib(REF_LIB))]
     except Exception as e:  # the reference build is not present
         return {"impl": "reference", "unavailable": f"reference build missing: {e}"}
-    sizes = {}
-    for name, bins, p in MODES:
-        d_cmp.zero_()
-        sizes[name] = ref.compress(d_in.data_ptr(), d_cmp.data_ptr(), dims, bins, p)
-        torch.cuda.synchronize()
-
-    def step():
-        for name, bins, p in MODES:
-            ref.compress(d_in.data_ptr(), d_cmp.data_ptr(), dims, bins, p)
-            ref.decompress(d_dec.data_ptr(), d_cmp.data_ptr(), sizes[name], dims, bins, p)
-
-    for _ in range(max(args.warmup, 3)):
-        step()
-    torch.cuda.synchronize()
+    try:
+        refs.append(("default arch (PTX JIT)", RefLib(REF_LIB_DEFAULT)))
+    except Exception:
+        pass
     stream = torch.cuda.current_stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    clocks = ClockSampler(torch.cuda.current_device())
-    clocks.start()
-    e0.record(stream)
-    for _ in range(args.steps):
-        step()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    clk = clocks.stop()
-    ms = e0.elapsed_time(e1) / args.steps
+
+    def run(ref, steps, clocks=None):
+        sizes = {}
+        for name, bins, p in MODES:
+            d_cmp.zero_()
+            sizes[name] = ref.compress(d_in.data_ptr(), d_cmp.data_ptr(), dims, bins, p)
+            torch.cuda.synchronize()
+
+        def step():
+            for name, bins, p in MODES:
+                ref.compress(d_in.data_ptr(), d_cmp.data_ptr(), dims, bins, p)
+                ref.decompress(d_dec.data_ptr(), d_cmp.data_ptr(), sizes[name], dims, bins, p)
+
+        for _ in range(max(args.warmup, 3)):
+            step()
+        torch.cuda.synchronize()
+        if clocks:
+            clocks.start()
+        e0.record(stream)
+        for _ in range(steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        clk = clocks.stop() if clocks else None
+        return e0.elapsed_time(e1) / steps, sizes, clk
+
+    builds = {}
+    for label, ref in refs[1:]:
+        ms_b, _, _ = run(ref, max(1, args.steps // 2))
+        builds[label] = round(ms_b, 4)
+    ms, sizes, clk = run(refs[0][1], args.steps, ClockSampler(torch.cuda.current_device()))
+    builds[refs[0][0]] = round(ms, 4)
+    label = min(builds, key=builds.get)
+    ref = dict(refs)[label]
+    if label != refs[0][0]:
+        # the faster build takes the timed steps again, clocks sampled
+        ms, sizes, clk = run(ref, args.steps, ClockSampler(torch.cuda.current_device()))
+        builds[label] = round(ms, 4)
     value = 4 * nbytes / (ms / 1e3) / 1e9
     e2e = None
     if args.e2e_steps > 0:
@@ -857,18 +1007,22 @@ def bench_reference_gpu(args, dims, dev, d_in, d_cmp, d_dec, nbytes, config, h):
                "h2d_bytes_per_step": int(moved["h2d"]), "d2h_bytes_per_step": int(moved["d2h"]),
                "ms_per_step": round(ems, 3),
                "path": "reference host API (cuLSZ_*_bsize64) with pinned host buffers copied in and out"}
+    per_config = None
+    if not args.no_per_config and args.dims is None and args.kind == "cssi":
+        per_config = bench_per_config(args, lambda kind, pdims: codec_ref(ref, pdims), torch.cuda.current_device())
     return {"impl": "reference",
             "metric": "lsCOMP compress+decompress throughput (lossless and lossy b=3 5 10 15 p=0.5), "
                       "uncompressed GB per second",
             "value": round(value, 2), "unit": "GB/s", "n_gpus": 1, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": round(ms, 4), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic (seeded CSSI-like generator)",
-            "config": config, "clocks": clk,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": data_note(args.kind),
+            "config": config, "clocks": clk, "build": label, "ms_per_step_by_build": builds,
             "cpu_baseline": {"value": round(value, 2), "unit": "GB/s", "cores": 1, "kind": "reference",
-                             "sample": "the reference's CUDA sources (nvcc -O3 sm_100a) through its host API on the "
-                                       "full stack; the reference has no CPU implementation (bench.py --impl "
-                                       "reference --ref-cpu times the C/OpenMP oracle on the host cores)"},
-            "e2e": e2e}
+                             "sample": f"the reference's CUDA sources ({label} build, the faster of the two) "
+                                       "through its host API on the full stack; the reference has no CPU "
+                                       "implementation (bench.py --impl reference --ref-cpu times the C/OpenMP "
+                                       "oracle on the host cores)"},
+            "e2e": e2e, "per_config": per_config}
 
 
 if __name__ == "__main__":

@@ -348,6 +348,19 @@ int lscomp_quality_u32(const uint32_t *d_ori, const uint32_t *d_dec, uint32_t x,
    run; allow = 1 (the default) restores tuning. */
 int lscomp_workspace_set_tuning(lscomp_workspace *ws, int allow);
 
+/* Failure injection for tests (no counterpart in the reference, whose
+   look-back spins without a bound, lsCOMP/src/cuLSZ_kernel.cu:1001-1004).
+   The next launch through this workspace starts its tile tickets at 1, so
+   tile 0 (decoder: segment 0 of the offsets kernel) is never claimed and
+   the look-back of its successor waits for a publication that never comes,
+   and every wait of that launch is limited to wait_ns (1 ms .. 2 s) instead
+   of 2 s.  The call returns LSCOMP_ERR_TIMEOUT after about that long; the
+   launch ends without a fault and the workspace serves the next call
+   normally.  Needs a stack of at least 2 tiles (decoder: 33 tiles) and a
+   workspace that does not tune (lscomp_workspace_set_tuning(ws, 0)), since
+   a tuning run would take the injected launch. */
+int lscomp_workspace_stall_next(lscomp_workspace *ws, uint64_t wait_ns);
+
 /* Wait for the workspace's last launch on `stream` and return its status. */
 int lscomp_workspace_check(lscomp_workspace *ws, void *stream);
 

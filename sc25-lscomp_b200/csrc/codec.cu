@@ -227,6 +227,14 @@ int lscomp_workspace_set_tuning(lscomp_workspace *ws, int allow)
     return LSCOMP_OK;
 }
 
+int lscomp_workspace_stall_next(lscomp_workspace *ws, uint64_t wait_ns)
+{
+    if (!ws || wait_ns < 1000000ull || wait_ns > 2000000000ull) return LSCOMP_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ws->mu);
+    ws->stall_wait_ns = wait_ns;
+    return LSCOMP_OK;
+}
+
 int lscomp_workspace_check(lscomp_workspace *ws, void *stream)
 {
     if (!ws) return LSCOMP_ERR_ARG;
@@ -347,7 +355,7 @@ extern "C" int lscomp_compress_u16_noalloc(const uint16_t *d_in, uint32_t x, uin
 {
     if (!d_in || !d_out) return LSCOMP_ERR_ARG;
     if (reinterpret_cast<uintptr_t>(d_in) % 2u || reinterpret_cast<uintptr_t>(d_out) % 4u) return LSCOMP_ERR_ARG;
-    EncArgs<uint16_t> a;
+    EncArgs<uint16_t> a = {};
     int layout = 0;
     if (!make_geom(x, y, z, Elem<uint16_t>::kTileBlocks, a.g) || !make_codec(bins, pooling, false, a.c, layout))
         return LSCOMP_ERR_ARG;

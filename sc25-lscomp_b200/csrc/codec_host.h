@@ -31,6 +31,11 @@ struct lscomp_workspace {
     bool no_tune = false;              // calls through this workspace never tune
     void *pipe = nullptr;              // host-memory calls: copy streams, slot buffers (host_pipe.cu)
     uint64_t host_chunk_bytes = 0;     // host-memory calls: input bytes per chunk (0: the default)
+    // lscomp_workspace_stall_next: the next launch starts its tile (or
+    // segment) tickets at 1 with this wait limit (ns), so tile 0 is never
+    // claimed and the look-back of tile 1 waits until the limit runs out
+    uint64_t stall_wait_ns = 0;
+    unsigned long long stall_words[2] = {0, 0};  // source of that launch's ticket and wait_ns
     std::mutex mu;
 };
 
@@ -170,6 +175,18 @@ inline int ws_prepare(lscomp_workspace *ws, uint64_t ntiles, cudaStream_t st)
     }
     ws->epoch++;
     cudaError_t e = cudaMemsetAsync(ws->ctl, 0, sizeof(LaunchCtl), st);
+    if (e == cudaSuccess && ws->stall_wait_ns) {
+        // one launch with tile 0 left unclaimed and a short wait limit
+        ws->stall_words[0] = 1;
+        ws->stall_words[1] = ws->stall_wait_ns;
+        ws->stall_wait_ns = 0;
+        e = cudaMemcpyAsync(&ws->ctl->ticket, &ws->stall_words[0], sizeof(unsigned long long),
+                            cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(&ws->ctl->wait_ns, &ws->stall_words[1], sizeof(unsigned long long),
+                                cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // the pageable source words are reused
+    }
     return cuda_status(e);
 }
 

@@ -29,7 +29,8 @@ struct LaunchCtl {
     unsigned int abort;          // set with error: every CTA stops waiting
     unsigned long long total;    // payload bytes of the stream (encoder)
     unsigned long long stream_len;
-    unsigned long long reserved[4];
+    unsigned long long wait_ns;  // limit of a single wait in ns (0: kWaitLimitNs)
+    unsigned long long reserved[3];
 };
 
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s for any single wait
@@ -57,6 +58,13 @@ __device__ __forceinline__ void raise_error(LaunchCtl *ctl, uint32_t code)
 __device__ __forceinline__ bool aborted(const LaunchCtl *ctl)
 {
     return *((volatile const unsigned int *)&ctl->abort) != 0u;
+}
+
+// The launch's limit for one wait (read when a wait starts to take long).
+__device__ __forceinline__ unsigned long long wait_limit(const LaunchCtl *ctl)
+{
+    const unsigned long long w = *((volatile const unsigned long long *)&ctl->wait_ns);
+    return w ? w : kWaitLimitNs;
 }
 
 // ---------------------------------------------------------------- mbarrier
@@ -105,11 +113,12 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, Launch
 {
     if (mbar_try_wait(bar, parity)) return true;
     const unsigned long long t0 = global_ns();
+    const unsigned long long limit = wait_limit(ctl);
     uint32_t spins = 0;
     while (!mbar_try_wait(bar, parity)) {
         if ((++spins & 31u) == 0) {
             if (aborted(ctl)) return false;
-            if (global_ns() - t0 > kWaitLimitNs) {
+            if (global_ns() - t0 > limit) {
                 raise_error(ctl, DEV_ERR_TIMEOUT);
                 return false;
             }
@@ -226,7 +235,7 @@ __device__ __forceinline__ unsigned long long lookback_warp(const unsigned long 
         ++spins;
         if ((spins & 63u) == 0) {
             bool stop = false;
-            if (lane == 0) stop = aborted(ctl) || (global_ns() - t0 > kWaitLimitNs);
+            if (lane == 0) stop = aborted(ctl) || (global_ns() - t0 > wait_limit(ctl));
             stop = __shfl_sync(0xffffffffu, stop, 0);
             if (stop) {
                 if (lane == 0) raise_error(ctl, DEV_ERR_TIMEOUT);
@@ -301,7 +310,7 @@ __device__ __forceinline__ unsigned long long lookback_floor(const unsigned long
         ++spins;
         if ((spins & 15u) == 0) {
             bool stop = false;
-            if (lane == 0) stop = aborted(ctl) || (global_ns() - t0 > kWaitLimitNs);
+            if (lane == 0) stop = aborted(ctl) || (global_ns() - t0 > wait_limit(ctl));
             stop = __shfl_sync(0xffffffffu, stop, 0);
             if (stop) {
                 if (lane == 0) raise_error(ctl, DEV_ERR_TIMEOUT);

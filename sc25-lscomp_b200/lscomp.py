@@ -153,6 +153,7 @@ def load_library() -> ctypes.CDLL:
     lib.lscomp_tune_report.argtypes = [ctypes.c_char_p, u64]
     lib.lscomp_tune_save.argtypes = [ctypes.c_char_p]
     lib.lscomp_tune_load.argtypes = [ctypes.c_char_p]
+    lib.lscomp_workspace_stall_next.argtypes = [vp, u64]
     _lib = lib
     return lib
 
@@ -203,6 +204,12 @@ class Workspace:
     def set_tuning(self, allow: bool) -> None:
         """False: calls through this workspace never run the tuner."""
         _check(load_library().lscomp_workspace_set_tuning(self._ws, 1 if allow else 0), "lscomp_workspace_set_tuning")
+
+    def stall_next(self, wait_ns: int) -> None:
+        """Failure injection: the next launch leaves tile 0 unclaimed and limits
+        every wait to wait_ns, so its look-back times out (LSCOMP_ERR_TIMEOUT)."""
+        _check(load_library().lscomp_workspace_stall_next(self._ws, ctypes.c_uint64(int(wait_ns))),
+               "lscomp_workspace_stall_next")
 
     def close(self):
         if self._ws:

@@ -28,17 +28,11 @@ def _noalloc(lib):
     return f
 
 
-def test_noalloc_matches_workspace_entry_point():
-    if not torch.cuda.is_available():
-        pytest.skip("no CUDA device")
-    import lscomp
+CASES = [((6, 333, 517), (1, 1, 1, 1), 1.0, 3), ((4, 250, 1030), (3, 5, 10, 15), 0.5, 4)]
 
-    lib = lscomp.load_library()
-    f = _noalloc(lib)
-    ws = lscomp.Workspace(0)
-    stream = torch.cuda.current_stream().cuda_stream
-    cases = [((6, 333, 517), (1, 1, 1, 1), 1.0, 3), ((4, 250, 1030), (3, 5, 10, 15), 0.5, 4)]
-    for dims, bins, p, seed in cases:  # two calls in a row
+
+def _compare(lscomp, lib, f, ws, stream):
+    for dims, bins, p, seed in CASES:  # two calls in a row
         a = lscomp.synth_cssi(dims, seed=seed)
         d_in = torch.from_numpy(a.view(np.int16)).cuda()
         cap = lscomp.max_stream_bytes(dims)
@@ -53,6 +47,39 @@ def test_noalloc_matches_workspace_entry_point():
         assert st == 0, lib.lscomp_status_string(st)
         assert (sl.value, rs.value) == (sl_w, rs_w)
         assert torch.equal(got[:sl_w], want[:sl_w])
+
+
+def test_noalloc_matches_workspace_entry_point():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import lscomp
+
+    lib = lscomp.load_library()
+    _compare(lscomp, lib, _noalloc(lib), lscomp.Workspace(0), torch.cuda.current_stream().cuda_stream)
+
+
+def test_noalloc_with_tuner_table_entries(tmp_path):
+    """The entry point takes the launch configuration the tuner's table holds
+    for its key (another tile size, or the 13-warp groups) when the tiles fit
+    its scratch; both calls must still write the same bytes."""
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import lscomp
+
+    lib = lscomp.load_library()
+    f = _noalloc(lib)
+    saved = tmp_path / "before.txt"
+    lscomp.tune_save(str(saved))
+    # keys "es layout pool kind vec bzb": the lossless case (layout 3, no
+    # pooling, 2-byte rows, 65 blocks per block-row) and the lossy one
+    # (increasing bins, pooling, 4-byte rows, 129 blocks per block-row)
+    for lossless_cfg, lossy_cfg in (("0 128", "2 256"), ("1 256", "0 128")):
+        table = tmp_path / "table.txt"
+        table.write_text(f"2 3 0 0 2 65 -> {lossless_cfg}\n2 1 1 0 4 129 -> {lossy_cfg}\n")
+        lscomp.tune_load(str(table))
+        _compare(lscomp, lib, f, lscomp.Workspace(0), torch.cuda.current_stream().cuda_stream)
+    lscomp.tune_clear()
+    lscomp.tune_load(str(saved))
 
 
 def test_noalloc_refuses_stacks_beyond_its_scratch():
