@@ -71,12 +71,13 @@ def parse():
     ap.add_argument("--no-per-config", action="store_true",
                     help="skip the XPCS-like and small stacks measured beside the default CSSI-like one")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--serve", type=float, default=0.0,
-                    help="serving benchmark: Poisson arrivals at this many requests per second (its own JSON line)")
-    ap.add_argument("--serve-seconds", type=float, default=10.0)
+    ap.add_argument("--serve", type=str, default="",
+                    help="serving benchmark: Poisson arrivals at this many requests per second, or a comma-separated "
+                         "sweep of rates (its own JSON line)")
+    ap.add_argument("--serve-seconds", type=float, default=60.0, help="duration of each rate of the serving run")
     ap.add_argument("--serve-max-mb", type=int, default=512, help="largest request of the serving benchmark")
-    ap.add_argument("--serve-arena-gb", type=int, default=32,
-                    help="device arena (and pinned staging) of the serving benchmark's server")
+    ap.add_argument("--serve-arena-gb", type=int, default=120,
+                    help="device arena of the serving benchmark's server (its admission cap)")
     ap.add_argument("--batch-frames", type=int, default=16, help="largest frame count of a batch stack")
     ap.add_argument("--ref-cpu", action="store_true",
                     help="with --impl reference: the oracle on the host cores instead of the reference's CUDA build")
@@ -488,65 +489,77 @@ def bench_serve(args, local):
             o = np.zeros(64 + lscomp.max_stream_bytes(dims), dtype=np.uint8)
             r = srv.wait(srv.submit_compress(a, dims, bins, p, o))
             conts[(k, name)] = o[: r["out_len"]].copy()
-    import threading
     import queue as qmod
 
-    pending = qmod.Queue()
-    lat, nbytes_done = [], [0]
+    # one output buffer per pool stack and direction, written before use, so
+    # the run measures the server and not page faults on fresh client memory
+    # (requests for the same stack may share one: their bytes are not checked)
+    outs = {k: (np.ones(64 + lscomp.max_stream_bytes(dims), dtype=np.uint8), np.ones_like(a))
+            for k, (dims, a) in enumerate(pool)}
 
-    def waiter():
+    def run_rate(rate, dur):
+        pending = qmod.Queue()
+        lat, nbytes_done, failed = [], [0], []
+
+        def waiter():
+            while True:
+                item = pending.get()
+                if item is None:
+                    return
+                rid, nb = item
+                r = srv.wait(rid)
+                if r["status"] != 0:
+                    failed.append(r)
+                lat.append((r["queued_ns"] + r["service_ns"]) / 1e6)
+                nbytes_done[0] += nb
+
+        st0 = srv.stats()
+        wt = threading.Thread(target=waiter)
+        wt.start()
+        t0 = time.perf_counter()
+        t_next = t0
+        n_sub = 0
         while True:
-            item = pending.get()
-            if item is None:
-                return
-            rid, nb = item
-            r = srv.wait(rid)
-            if r["status"] != 0:
-                raise SystemExit(f"request failed: {r}")
-            lat.append((r["queued_ns"] + r["service_ns"]) / 1e6)
-            nbytes_done[0] += nb
+            t_next += float(rng.exponential(1.0 / rate))
+            if t_next - t0 > dur:
+                break
+            while time.perf_counter() < t_next:
+                pass
+            k = int(rng.integers(0, len(pool)))
+            dims, a = pool[k]
+            name, bins, p = modes[0] if rng.random() < 0.6 else modes[1]
+            if rng.random() < 0.7:
+                rid = srv.submit_compress(a, dims, bins, p, outs[k][0])
+            else:
+                rid = srv.submit_decompress(conts[(k, name)], outs[k][1])
+            pending.put((rid, a.nbytes))
+            n_sub += 1
+        pending.put(None)
+        wt.join()
+        elapsed = time.perf_counter() - t0
+        if failed:
+            raise SystemExit(f"request failed: {failed[0]}")
+        st = srv.stats()
+        lat_a = np.array(lat)
+        return {"offered_req_per_s": rate, "achieved_req_per_s": round(n_sub / elapsed, 1), "requests": n_sub,
+                "p50_ms": round(float(np.percentile(lat_a, 50)), 3),
+                "p99_ms": round(float(np.percentile(lat_a, 99)), 3), "mean_ms": round(float(lat_a.mean()), 3),
+                "input_gb_per_s": round(nbytes_done[0] / elapsed / 1e9, 2),
+                "launch_rounds": st["rounds"] - st0["rounds"], "batches": st["batches"] - st0["batches"],
+                "batched_requests": st["batched_requests"] - st0["batched_requests"]}
 
-    wt = threading.Thread(target=waiter)
-    wt.start()
-    rate, dur = args.serve, args.serve_seconds
-    t0 = time.perf_counter()
-    t_next = t0
-    n_sub = 0
-    while True:
-        t_next += float(rng.exponential(1.0 / rate))
-        if t_next - t0 > dur:
-            break
-        while time.perf_counter() < t_next:
-            pass
-        k = int(rng.integers(0, len(pool)))
-        dims, a = pool[k]
-        name, bins, p = modes[0] if rng.random() < 0.6 else modes[1]
-        if rng.random() < 0.7:
-            o = np.empty(64 + lscomp.max_stream_bytes(dims), dtype=np.uint8)
-            rid = srv.submit_compress(a, dims, bins, p, o)
-        else:
-            o = np.empty_like(a)
-            rid = srv.submit_decompress(conts[(k, name)], o)
-        pending.put((rid, a.nbytes))
-        n_sub += 1
-    pending.put(None)
-    wt.join()
-    elapsed = time.perf_counter() - t0
-    st = srv.stats()
+    rates = [float(v) for v in str(args.serve).split(",")]
+    sweep = [run_rate(r, args.serve_seconds) for r in rates]
     srv.close()
-    lat_a = np.array(lat)
+    head = sweep[0]
     print(json.dumps({"metric": "serving latency p99 (Poisson arrivals, host buffers in and out)",
-                      "value": round(float(np.percentile(lat_a, 99)), 3), "unit": "ms", "higher_is_better": False,
-                      "p50_ms": round(float(np.percentile(lat_a, 50)), 3),
-                      "p99_ms": round(float(np.percentile(lat_a, 99)), 3),
-                      "mean_ms": round(float(lat_a.mean()), 3), "requests": n_sub,
-                      "offered_req_per_s": rate, "achieved_req_per_s": round(n_sub / elapsed, 1),
-                      "input_gb_per_s": round(nbytes_done[0] / elapsed / 1e9, 2),
-                      "rounds": st["rounds"], "batches": st["batches"], "batched_requests": st["batched_requests"],
+                      "value": head["p99_ms"], "unit": "ms", "higher_is_better": False, **head,
+                      "sweep": sweep if len(sweep) > 1 else None,
                       "config": {"workload": f"32 seeded stacks, log-uniform 256 KB..{args.serve_max_mb} MB, "
                                              "1024x1024 (XPCS-like) or 1813x1558 (CSSI-like) uint16 frames; 70/30 "
                                              "compress/decompress; 60/40 lossless/lossy", "arena_bytes": arena,
-                                 "duration_s": dur}}))
+                                 "duration_s_per_rate": args.serve_seconds,
+                                 "copy_threads_per_direction": int(os.environ.get("LSCOMP_SERVER_COPY_THREADS", 4))}}))
 
 
 def main():

@@ -297,24 +297,36 @@ int lscomp_decompress_container(lscomp_workspace *ws, const uint8_t *d_in, uint6
                                 uint64_t out_cap, lscomp_container_info *info, void *stream);
 
 /* Serving loop (no counterpart in the reference).  A server owns a device
-   arena of arena_bytes, pinned staging of the same size, a workspace, a
-   CUDA stream and a worker thread.  Any thread submits requests with host
-   buffers; the worker admits waiting requests in arrival order while their
-   worst-case device footprints (input + largest possible output) fit the
-   arena, sends the compress requests of a round that share element type,
-   bins and pooling threshold to the GPU as one batch launch, and decodes
-   the decompress requests.  A compress request produces a container (see
-   above) in h_out; a decompress request takes a container.  Outputs do not
-   depend on what else is in the batch.  Submit returns a request id > 0, or
-   minus a status (LSCOMP_ERR_TOO_LARGE: the footprint exceeds the arena).
-   Caller buffers must stay valid until lscomp_server_wait returns for the
-   request; wait releases the request.  destroy runs what was submitted. */
+   arena of arena_bytes, 2 x 128 MB of pinned staging (whatever the arena's
+   size), a workspace, three CUDA streams and three pipeline threads.  Any
+   thread submits requests with host buffers.  The uploader admits waiting
+   requests in arrival order as soon as the arena has room for a request's
+   worst-case device footprint (input + largest possible output) and copies
+   its input up; the launcher runs every request uploaded so far as batch
+   launches (the compress requests of one element type as one launch, each
+   stack with its own shape, bins and pooling threshold; the decompress
+   requests of one element type as another) and, when a batch fails, runs
+   its requests again one at a time so a bad request fails alone; the
+   downloader copies each output down and releases its arena space.  So
+   requests that arrive while others are on the GPU are admitted as memory
+   frees, and their copies overlap the kernels of others.  A compress
+   request produces a container (see above) in h_out; a decompress request
+   takes a container.  Outputs do not depend on what else is in the batch.
+   Submit returns a request id > 0, or minus a status (LSCOMP_ERR_TOO_LARGE:
+   the footprint exceeds the arena).  Caller buffers must stay valid until
+   lscomp_server_wait returns for the request; one thread waits for a given
+   request (a second waiter gets LSCOMP_ERR_ARG), and wait releases it.
+   destroy runs what was submitted.  Environment: LSCOMP_SERVER_COPY_THREADS
+   (default 4) host threads per direction copy between caller buffers and
+   staging. */
 typedef struct lscomp_server lscomp_server;
 typedef struct lscomp_server_result {
     int status;          /* LSCOMP_OK or the request's error */
     uint64_t out_len;    /* bytes written to h_out */
     uint64_t queued_ns;  /* submit -> admitted */
     uint64_t service_ns; /* admitted -> done (copies, kernels, copies) */
+    uint64_t admit_ns;   /* when it was admitted and when it was done, on the */
+    uint64_t done_ns;    /* host's monotonic clock (ns): compare requests */
 } lscomp_server_result;
 
 int lscomp_server_create(lscomp_server **server, int device, uint64_t arena_bytes);

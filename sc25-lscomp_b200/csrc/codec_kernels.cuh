@@ -1534,20 +1534,17 @@ __device__ __forceinline__ void dec_load(const uint8_t *src, uint32_t h, uint32_
     }
 }
 
-// Values of one unit from its plane words: transposes back, pooled rows
-// expanded, de-quantised, stored to rows r and r+4 of block b.
-template <typename T, int VEC>
-__device__ __forceinline__ void dec_unit(const DecArgs<T> &a, const TileInfo &ti, const DecSmem &sm, uint32_t Y[][4],
-                                         uint32_t h, uint32_t b, uint32_t r, unsigned long long ebase)
+// Values of rows r (A) and r+4 (B) of this lane's block from the unit's
+// plane words: transposes back, pooled rows expanded, de-quantised by the
+// header's bin.  All 32 lanes of the warp take part (one unit).
+template <typename T>
+__device__ __forceinline__ void dec_values(uint32_t Y[][4], uint32_t h, bool active, uint32_t r, uint32_t bin,
+                                           Row<T> &A, Row<T> &B)
 {
     constexpr int NW = Elem<T>::kWords;
     constexpr int NG = Elem<T>::kGroups;
-    const Geom &g = a.g;
     const bool even = (r & 1u) == 0;
-    const bool active = b < ti.nblk;
-    SegLoc L = seg_locate<T, false>(g, ti, sm.br_rel, sm.br_rows, nullptr, nullptr, active ? b : 0, r);
     const bool pool = (h & 0x80u) != 0;
-    const uint32_t bin = a.c.bins[(h >> 5) & 3u];
     const uint32_t wrate = __reduce_max_sync(0xffffffffu, h & 0x1fu);
     const XSel xs = xsel(r);
     // plane bytes per byte group, back in row order: [grp][0/1] = lo/hi half
@@ -1568,7 +1565,6 @@ __device__ __forceinline__ void dec_unit(const DecArgs<T> &a, const TileInfo &ti
         PA[grp][1] = xpose4(y3, xs);
         PB[grp][1] = xpose4(Y[grp][3], xs);
     }
-    Row<T> A, B;
     row_values(PA, A, wrate);
     row_values(PB, B, wrate);
     if (__any_sync(0xffffffffu, active && pool)) {
@@ -1591,6 +1587,19 @@ __device__ __forceinline__ void dec_unit(const DecArgs<T> &a, const TileInfo &ti
         dequant(A, bin);
         dequant(B, bin);
     }
+}
+
+// Values of one unit from its plane words (dec_values), stored to rows r
+// and r+4 of block b.
+template <typename T, int VEC>
+__device__ __forceinline__ void dec_unit(const DecArgs<T> &a, const TileInfo &ti, const DecSmem &sm, uint32_t Y[][4],
+                                         uint32_t h, uint32_t b, uint32_t r, unsigned long long ebase)
+{
+    const Geom &g = a.g;
+    const bool active = b < ti.nblk;
+    SegLoc L = seg_locate<T, false>(g, ti, sm.br_rel, sm.br_rows, nullptr, nullptr, active ? b : 0, r);
+    Row<T> A, B;
+    dec_values<T>(Y, h, active, r, a.c.bins[(h >> 5) & 3u], A, B);
     if (active) {
         T *rowA = a.out + ebase + L.growA;
         if (r < L.nrows) store8<VEC>(rowA, A, L.ncols);

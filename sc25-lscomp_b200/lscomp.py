@@ -65,7 +65,7 @@ class ContainerInfo(ctypes.Structure):
 class ServerResult(ctypes.Structure):
     """struct lscomp_server_result of include/lscomp.h."""
     _fields_ = [("status", ctypes.c_int), ("out_len", ctypes.c_uint64), ("queued_ns", ctypes.c_uint64),
-                ("service_ns", ctypes.c_uint64)]
+                ("service_ns", ctypes.c_uint64), ("admit_ns", ctypes.c_uint64), ("done_ns", ctypes.c_uint64)]
 
 
 class LscompStack(ctypes.Structure):
@@ -575,7 +575,7 @@ class Server:
         _check(load_library().lscomp_server_wait(self._h, ctypes.c_int64(rid), ctypes.byref(r)), "lscomp_server_wait")
         self._keep.pop(rid, None)
         return {"status": r.status, "out_len": int(r.out_len), "queued_ns": int(r.queued_ns),
-                "service_ns": int(r.service_ns)}
+                "service_ns": int(r.service_ns), "admit_ns": int(r.admit_ns), "done_ns": int(r.done_ns)}
 
     def stats(self) -> dict:
         a, b, c = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()

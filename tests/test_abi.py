@@ -65,3 +65,19 @@ def test_status_strings():
     lib.lscomp_status_string.restype = ctypes.c_char_p
     for s in range(8):
         assert lib.lscomp_status_string(s)
+
+
+# host-side launch stubs of the four __global__ kernels of
+# lsCOMP/include/cuLSZ_kernel.h:9-36 (include/cuLSZ_kernel.h)
+REFERENCE_KERNELS = [
+    "_Z39cuLSZ_compression_kernel_uint16_bsize64PKtPhPVmS3_PVij5uint35uint4f",
+    "_Z41cuLSZ_decompression_kernel_uint16_bsize64PtPKhPVmS3_PVij5uint35uint4f",
+    "_Z39cuLSZ_compression_kernel_uint32_bsize64PKjPhPVjS3_PVij5uint35uint4f",
+    "_Z41cuLSZ_decompression_kernel_uint32_bsize64PjPKhPVjS3_PVij5uint35uint4f",
+]
+
+
+def test_reference_kernel_header_exported():
+    syms = exported()
+    missing = [m for m in REFERENCE_KERNELS if m not in syms]
+    assert not missing, missing

@@ -136,3 +136,68 @@ def test_threads(lz):
         assert r["status"] == 0
         assert np.array_equal(o[: r["out_len"]], alone(lz, ws, a, d, b, p))
     srv.close()
+
+
+def test_bad_request_fails_alone(lz):
+    """A uint32 request whose quotient needs 32 bit planes (the 5-bit rate
+    field cannot say so: LSCOMP_ERR_RANGE) is batched with valid requests;
+    only it fails, and the others' containers equal the single calls'."""
+    reqs = requests(12, seed=4)
+    bad = np.zeros((1, 8, 8), dtype=np.uint32)
+    bad[0, 0, 0] = 0xFFFFFFFF
+    ws = lz.Workspace(0)
+    srv = lz.Server(0, arena_bytes=1 << 30)
+    # two uint32 requests around the bad one, so it shares their batch
+    reqs.insert(3, (bad, bad.shape, LOSSLESS[0], 1.0))
+    reqs.insert(2, (stack((2, 17, 33), 77, wide=True), (2, 17, 33), *LOSSY))
+    reqs.insert(5, (stack((1, 40, 9), 78, wide=True), (1, 40, 9), *LOSSLESS))
+    outs = [np.zeros(64 + lz.max_stream_bytes(d, a.itemsize), dtype=np.uint8) for a, d, _, _ in reqs]
+    ids = [srv.submit_compress(a, d, b, p, o) for (a, d, b, p), o in zip(reqs, outs)]
+    res = [srv.wait(i) for i in ids]
+    for (a, d, b, p), o, r in zip(reqs, outs, res):
+        if a is bad:
+            assert r["status"] == 6 and r["out_len"] == 0
+        else:
+            assert r["status"] == 0
+            assert np.array_equal(o[: r["out_len"]], alone(lz, ws, a, d, b, p))
+    srv.close()
+
+
+def test_admitted_while_others_in_flight(lz):
+    """A request submitted while a large one is being served is admitted
+    (and so starts its upload) before the large one completes."""
+    srv = lz.Server(0, arena_bytes=4 << 30)
+    big = np.random.default_rng(9).integers(0, 50, size=(64, 1024, 1024), dtype=np.uint16)  # 128 MB
+    small = stack((1, 64, 64), 10)
+    ob = np.zeros(64 + lz.max_stream_bytes(big.shape), dtype=np.uint8)
+    os_ = np.zeros(64 + lz.max_stream_bytes(small.shape), dtype=np.uint8)
+    rb = srv.submit_compress(big, big.shape, *LOSSY, ob)
+    rs = srv.submit_compress(small, small.shape, *LOSSLESS, os_)
+    r_small, r_big = srv.wait(rs), srv.wait(rb)
+    assert r_small["status"] == 0 and r_big["status"] == 0
+    assert r_small["admit_ns"] < r_big["done_ns"]
+    srv.close()
+
+
+def test_second_waiter_refused(lz):
+    """Two threads wait for the same request: one gets the result, the other
+    LSCOMP_ERR_ARG (while the first waits, or after it released the request)."""
+    srv = lz.Server(0, arena_bytes=1 << 30)
+    a = np.random.default_rng(12).integers(0, 50, size=(32, 1024, 1024), dtype=np.uint16)
+    o = np.zeros(64 + lz.max_stream_bytes(a.shape), dtype=np.uint8)
+    rid = srv.submit_compress(a, a.shape, *LOSSLESS, o)
+    got = []
+
+    def waiter():
+        try:
+            got.append(srv.wait(rid)["status"])
+        except lz.LscompError as e:
+            got.append(-e.status)
+
+    th = [threading.Thread(target=waiter) for _ in range(2)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    assert sorted(got) == [-1, 0]
+    srv.close()
