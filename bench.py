@@ -78,7 +78,7 @@ def parse():
     ap.add_argument("--serve-max-mb", type=int, default=512, help="largest request of the serving benchmark")
     ap.add_argument("--serve-arena-gb", type=int, default=120,
                     help="device arena of the serving benchmark's server (its admission cap)")
-    ap.add_argument("--batch-frames", type=int, default=16, help="largest frame count of a batch stack")
+    ap.add_argument("--batch-frames", type=int, default=64, help="largest frame count of a batch stack")
     ap.add_argument("--ref-cpu", action="store_true",
                     help="with --impl reference: the oracle on the host cores instead of the reference's CUDA build")
     ap.add_argument("--ref-step-seconds", type=float, default=1.5,
@@ -301,51 +301,122 @@ def batch_workload(n, max_frames, seed=11):
     return out
 
 
+POOL_FRAMES = 64   # frames per kind in the device frame pools of the batch benchmark
+POOL_SIDE = 2048  # their height and width (the largest a batch stack has)
+
+
+def batch_pools(lscomp, dev, frames, seed=11):
+    """Seeded CSSI-like and XPCS-like frames (at least POOL_FRAMES, and at
+    least a stack's largest frame count, of POOL_SIDE^2 each) made by the
+    host generators and kept on the device; batch stacks are cut from them
+    (batch_assemble)."""
+    import torch
+
+    dims = (max(POOL_FRAMES, frames), POOL_SIDE, POOL_SIDE)
+    return {k: torch.from_numpy(getattr(lscomp, f"synth_{k}")(dims, seed=seed + i).view(np.int16)).to(dev).view(dims)
+            for i, k in enumerate(("cssi", "xpcs"))}
+
+
+def batch_assemble(pools, d, dst):
+    """Stack d (frames F, height H, width W) into dst: F consecutive pool
+    frames of its kind (so the XPCS-like frames keep their frame-to-frame
+    correlation), each cut to its central H x W window."""
+    f, h, w = d["dims"]
+    o = d["seed"] % (pools[d["kind"]].shape[0] - f + 1)
+    y0, x0 = (POOL_SIDE - h) // 2, (POOL_SIDE - w) // 2
+    dst.view(f, h, w).copy_(pools[d["kind"]][o:o + f, y0:y0 + h, x0:x0 + w])
+
+
 def bench_batch(args, local):
     """Batched compress of many uneven stacks, each with its own bins and
     pooling threshold: one lscomp_compress_batch_ex_u16 call, and the same
     captured once as a CUDA graph (lscomp_plan_*), against one plain call
     per stack and one plain call per frame (and, for --impl reference, the
-    reference's host API called per stack).  Inputs resident in HBM; each
-    stack is generated on the host and copied to its slice of one device
-    buffer, so host memory holds one stack at a time."""
+    reference's host API called per stack); then batch decompression of all
+    streams against one plain call per stack.  Inputs resident in HBM.
+
+    Stacks are cut on the device from frame pools (batch_pools), and every
+    output buffer has the exact size of its stream (lscomp_stream_sizes_batch,
+    a pass that writes nothing), so the configuration's 2000 stacks of up to
+    64 frames fit one GPU; if they do not fit the free device memory, the
+    largest leading subset that does is run, and the line says so.  The
+    decodes are written over the inputs once compression is measured."""
     import torch
+
+    import lscomp
 
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream()
+    ws = lscomp.Workspace(local)
     desc = batch_workload(args.batch, args.batch_frames)
+    t_setup = time.perf_counter()
+    pools = batch_pools(lscomp, dev, args.batch_frames)
+
+    def n_el(d):
+        return d["dims"][0] * d["dims"][1] * d["dims"][2]
+
+    def al16(nbytes):
+        return (nbytes + 15) // 16 * 16
+
+    # exact stream sizes, stack by stack through a bounded scratch buffer
+    exact = [0] * len(desc)
+    scratch_el = 4 << 30
+    buf = torch.empty(scratch_el, dtype=torch.int16, device=dev)
+    i = 0
+    while i < len(desc):
+        items, off = [], 0
+        while i < len(desc) and off + al16(2 * n_el(desc[i])) // 2 <= scratch_el:
+            d = desc[i]
+            sl = buf[off:off + n_el(d)]
+            batch_assemble(pools, d, sl)
+            items.append((sl, d["dims"], None, d["bins"], d["p"]))
+            off += al16(2 * n_el(d)) // 2
+            i += 1
+        for k, v in enumerate(lscomp.stream_sizes_batch(ws, items)):
+            exact[i - len(items) + k] = v
+    del buf, items
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    # the largest leading subset whose inputs and exact outputs fit
+    free, _ = torch.cuda.mem_get_info(dev)
+    frame_scratch = max(lscomp.max_stream_bytes((1, d["dims"][1], d["dims"][2])) for d in desc)
+    budget = free - (6 << 30) - frame_scratch - 2 * max(al16(lscomp.max_stream_bytes(d["dims"])) for d in desc)
+    n, used = 0, 0
+    while n < len(desc) and used + al16(2 * n_el(desc[n])) + al16(exact[n]) <= budget:
+        used += al16(2 * n_el(desc[n])) + al16(exact[n])
+        n += 1
+    desc = desc[:n]
     frames = sum(d["dims"][0] for d in desc)
-    nel = [d["dims"][0] * d["dims"][1] * d["dims"][2] for d in desc]
+    nel = [n_el(d) for d in desc]
     nbytes = 2 * sum(nel)
-
-    def cap_of(dims):
-        nb = dims[0] * ((dims[1] + 7) // 8) * ((dims[2] + 7) // 8)
-        return (nb + 3) // 4 * 4 + 128 * nb
-
     offs_in, offs_out, n_in, n_out = [], [], 0, 0
-    for d, n in zip(desc, nel):
+    for d, ne, ex in zip(desc, nel, exact):
         offs_in.append(n_in)
-        n_in += (n + 7) // 8 * 8  # each stack at a 16-byte boundary
+        n_in += al16(2 * ne) // 2
         offs_out.append(n_out)
-        n_out += (cap_of(d["dims"]) + 15) // 16 * 16
+        n_out += al16(ex)
     d_in_all = torch.empty(n_in, dtype=torch.int16, device=dev)
     d_out_all = torch.zeros(n_out, dtype=torch.uint8, device=dev)
-    import lscomp
-
     items = []
-    for d, n, oi, oo in zip(desc, nel, offs_in, offs_out):
-        h = getattr(lscomp, f"synth_{d['kind']}")(d["dims"], seed=d["seed"])
-        d_in = d_in_all[oi:oi + n]
-        d_in.copy_(torch.from_numpy(h.view(np.int16).ravel()))
-        items.append((d_in, d["dims"], d_out_all[oo:oo + cap_of(d["dims"])], d["bins"], d["p"]))
-    del h
+    for d, ne, oi, oo, ex in zip(desc, nel, offs_in, offs_out, exact):
+        d_in = d_in_all[oi:oi + ne]
+        batch_assemble(pools, d, d_in)
+        items.append((d_in, d["dims"], d_out_all[oo:oo + ex], d["bins"], d["p"]))
+    del pools
     torch.cuda.synchronize()
+    t_setup = time.perf_counter() - t_setup
     config = {"workload": f"{len(desc)} stacks, frames U{{1..{args.batch_frames}}}, frame height and width "
                           f"U{{100..2048}} uint16, CSSI-like and XPCS-like alternating; per stack bins from "
                           f"{{lossless, 3 5 10 15, 5 10 15 20}} and p from {{0.3, 0.5, 0.8}} (lossless: p 1)",
-              "frames": frames, "input_bytes": nbytes,
-              "scaled_from": "2000 stacks with frames U{1..64} (about 150 GB of input, more than one GPU holds "
-                             "with worst-case stream buffers); frames per stack reduced"}
+              "stacks": len(desc), "stacks_asked": args.batch, "frames": frames, "input_bytes": nbytes,
+              "stream_bytes": int(sum(exact[:n])),
+              "data": f"stacks cut on the device from {POOL_FRAMES} seeded frames per kind "
+                      f"({POOL_SIDE}x{POOL_SIDE}, host generators): consecutive frames, central window",
+              "output_buffers": "exact stream sizes from lscomp_stream_sizes_batch_u16",
+              "setup_s": round(t_setup, 1)}
+    if n < args.batch:
+        config["subset"] = (f"the first {n} of {args.batch} stacks: their inputs and exact outputs fill the "
+                            "free device memory")
 
     def timed(fn, reps):
         for _ in range(max(args.warmup, 3)):
@@ -380,12 +451,15 @@ def bench_batch(args, local):
                           "per_stack_calls_ms": round(ms, 3), "config": config}))
         return
 
-    ws = lscomp.Workspace(local)
+    t0 = time.perf_counter()
+    lscomp.stream_sizes_batch(ws, items)
+    t_sizes = (time.perf_counter() - t0) * 1e3
     got = lscomp.compress_batch_mixed(ws, items)
+    assert [sl for sl, _ in got] == exact[:n], "size pass differs from the written streams"
     step = max(1, len(items) // 24)
+    chk = torch.empty(max(lscomp.max_stream_bytes(it[1]) for it in items[::step]), dtype=torch.uint8, device=dev)
     for it, (sl, rs) in zip(items[::step], got[::step]):
         d_in, dims, d_out, bins, p = it
-        chk = torch.zeros(d_out.numel(), dtype=torch.uint8, device=dev)
         assert lscomp.compress_into(ws, d_in, dims, bins, p, chk) == (sl, rs)
         assert torch.equal(chk[:sl], d_out[:sl]), "batch stream differs from the single-stack stream"
     t_batch = timed(lambda: lscomp.compress_batch_mixed(ws, items), args.steps)
@@ -401,8 +475,7 @@ def bench_batch(args, local):
     t_stack = timed(loop_stack, args.steps)
     # one plain call per frame, each frame a stack of its own; every frame
     # writes the same scratch stream buffer (only the time is kept)
-    scratch = torch.empty(max(lscomp.max_stream_bytes((1, d["dims"][1], d["dims"][2])) for d in desc),
-                          dtype=torch.uint8, device=dev)
+    scratch = torch.empty(frame_scratch, dtype=torch.uint8, device=dev)
 
     def loop_frame():
         for d_in, dims, d_out, bins, p in items:
@@ -411,16 +484,22 @@ def bench_batch(args, local):
                 lscomp.compress_into(ws, d_in[f * fsz:(f + 1) * fsz], (1, dims[1], dims[2]), bins, p, scratch)
 
     t_frame = timed(loop_frame, max(1, args.steps // 2))
-    # decode every stream back: one batch-decompression call against one
-    # plain call per stack (outputs in a third buffer; checked against the
-    # inputs for the lossless stacks)
-    d_dec_all = torch.empty_like(d_in_all)
-    ditems = [(d_out, sl, dims, d_dec_all[oi:oi + (d_in.numel())], bins, p)
-              for (d_in, dims, d_out, bins, p), (sl, _), oi in zip(items, got, offs_in)]
-    lscomp.decompress_batch(ws, ditems)
-    for (d_in, dims, d_out, bins, p), dit in zip(items[::step], ditems[::step]):
+    del scratch
+    # decode every stream: first the sampled stacks into a scratch buffer,
+    # checked (lossless: the input; lossy: the single-stack decode), then
+    # all of them over the inputs (no longer needed), one batch call against
+    # one plain call per stack
+    dchk = torch.empty(max(it[0].numel() for it in items[::step]), dtype=torch.int16, device=dev)
+    for (d_in, dims, d_out, bins, p), (sl, _) in zip(items[::step], got[::step]):
+        ne = d_in.numel()
+        lscomp.decompress_batch(ws, [(d_out, sl, dims, dchk[:ne], bins, p)])
         if bins == (1, 1, 1, 1):
-            assert torch.equal(dit[3], d_in), "batch decode differs from the input (lossless)"
+            assert torch.equal(dchk[:ne], d_in), "batch decode differs from the input (lossless)"
+        one = torch.empty_like(d_in)
+        lscomp.decompress_into(ws, d_out, sl, dims, bins, p, one)
+        assert torch.equal(dchk[:ne], one), "batch decode differs from the single-stack decode"
+    del dchk
+    ditems = [(d_out, sl, dims, d_in, bins, p) for (d_in, dims, d_out, bins, p), (sl, _) in zip(items, got)]
     t_dbatch = timed(lambda: lscomp.decompress_batch(ws, ditems), args.steps)
 
     def loop_dstack():
@@ -429,8 +508,10 @@ def bench_batch(args, local):
 
     t_dstack = timed(loop_dstack, args.steps)
     res = {"batch_call_ms": round(t_batch, 3), "graph_plan_ms": round(t_plan, 3),
+           "size_pass_ms": round(t_sizes, 3),
            "decompress_batch_call_ms": round(t_dbatch, 3), "decompress_per_stack_calls_ms": round(t_dstack, 3),
            "decompress_frames_per_s": {"batch_call": fps(t_dbatch), "per_stack_calls": fps(t_dstack)},
+           "decompress_output_gbs_batch_call": round(nbytes / t_dbatch / 1e6, 1),
            "per_stack_calls_ms": round(t_stack, 3), "per_frame_calls_ms": round(t_frame, 3),
            "frames_per_s": {"graph_plan": fps(t_plan), "batch_call": fps(t_batch), "per_stack_calls": fps(t_stack),
                             "per_frame_calls": fps(t_frame)},

@@ -20,6 +20,14 @@
 #include <stddef.h>
 #include <cuda_runtime.h>
 
+/* Stream capacity: these functions take none, like the reference's, and
+   treat d_cmpBytes as holding the worst-case stream -- roundup4(nb) + 128 nb
+   bytes for uint16, roundup4(nb) + 248 nb for uint32, nb = X ceil(Y/8)
+   ceil(Z/8) (lscomp_max_stream_bytes_u16/_u32 in lscomp.h).  A caller that
+   allocates less (the reference's CLIs allocate X Y Z sizeof(T) bytes,
+   lsCOMP/example/lsCOMP_xpcs.cpp:137, which is smaller for incompressible
+   data) is not protected from an overrun, exactly as with the reference;
+   the C ABI's calls take the capacity and refuse instead of overrunning. */
 void cuLSZ_compression_uint32_bsize64(uint32_t* d_oriData, unsigned char* d_cmpBytes, size_t* cmpSize, uint3 dims, uint4 quantBins, float poolingSH, cudaStream_t stream=0);
 void cuLSZ_decompression_uint32_bsize64(uint32_t* d_decData, unsigned char* d_cmpBytes, size_t cmpSize, uint3 dims, uint4 quantBins, float poolingSH, cudaStream_t stream=0);
 void cuLSZ_compression_uint16_bsize64(uint16_t* d_oriData, unsigned char* d_cmpBytes, size_t* cmpSize, uint3 dims, uint4 quantBins, float poolingSH, cudaStream_t stream=0);

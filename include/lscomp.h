@@ -201,6 +201,20 @@ int lscomp_decompress_batch_u16(lscomp_workspace *ws, const lscomp_stack *stacks
 int lscomp_decompress_batch_u32(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, const uint32_t *bins,
                                 const float *pooling, void *stream);
 
+/* Exact stream sizes of a batch (no counterpart in the reference): for each
+   stack, the number of bytes lscomp_compress_batch_ex_* (or the single-stack
+   call) would write with bins[4 i .. 4 i + 3] and pooling[i] -- the header,
+   its pad and the payload -- computed by one pass over the inputs that
+   writes no stream, so output buffers can be allocated to size instead of
+   at the worst case (lscomp_max_stream_bytes_*, about the input's size).
+   Only d_in and x, y, z of each stack are used.  A uint32 quotient that
+   needs 32 bit planes fails with LSCOMP_ERR_RANGE as compression would.
+   Synchronises the stream. */
+int lscomp_stream_sizes_batch_u16(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, const uint32_t *bins,
+                                  const float *pooling, uint64_t *stream_len, void *stream);
+int lscomp_stream_sizes_batch_u32(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, const uint32_t *bins,
+                                  const float *pooling, uint64_t *stream_len, void *stream);
+
 /* Graph plans (no counterpart in the reference).  A plan fixes one
    compression -- n stacks (n = 1: the single-stack kernel, n > 1: the batch
    kernel), their buffers and shapes, bins and pooling threshold -- and

@@ -138,9 +138,11 @@ int compress_batch_t(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t 
         if (!make_geom(q.x, q.y, q.z, Elem<T>::kTileBlocks, g)) return LSCOMP_ERR_ARG;
         if (q.cap < g.R) return LSCOMP_ERR_CAPACITY;
         const int v = vec_class(q.d_in, q.z, sizeof(T));
-        if (v < vec) vec = v;
+        if (sizeof(T) == 4 && v == 2) return LSCOMP_ERR_ARG;
     }
-    if (sizeof(T) == 4 && vec == 2) return LSCOMP_ERR_ARG;
+    // every stack is read with its own row access width (Geom::vec); the
+    // launch is instantiated once for all widths
+    vec = sizeof(T) == 2 ? 2 : 4;
     cudaStream_t st = (cudaStream_t)stream;
     std::lock_guard<std::mutex> lk(ws->mu);
     int prev = 0;
@@ -160,6 +162,7 @@ int compress_batch_t(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t 
             for (uint32_t s = 0; s < n; s++) {
                 BatchStack &b = ws->h_stacks[s];
                 b.g = geom[s];
+                b.g.vec = (uint32_t)vec_class(stacks[s].d_in, stacks[s].z, sizeof(T));
                 b.c = codec[s];
                 b.in = stacks[s].d_in;
                 b.out = stacks[s].d_out;
@@ -210,6 +213,150 @@ int compress_batch_t(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t 
     return r;
 }
 
+// ---------------------------------------------------------------- stream sizes
+// The exact stream length of every stack of a batch without writing any
+// stream: pass A of the encoder (every block's header byte, the same
+// block_header as enc_compute, so the same sizes) summed per stack.  One CTA
+// per tile at a time, rows read straight from global memory with each
+// stack's row access width; a tile's sum goes to its stack's counter with
+// one atomic add.
+template <typename T, int BINS, bool POOL>
+__global__ void __launch_bounds__(kThreads) size_kernel(const BatchStack *stacks, const uint32_t *tile_stack,
+                                                        unsigned long long ntiles, unsigned long long *payload,
+                                                        LaunchCtl *ctl)
+{
+    __shared__ BatchStack bs;
+    __shared__ uint32_t sum_s, bad_s, stk_s;
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, jb = lane & 7u, r = lane >> 3;
+    for (unsigned long long gt = blockIdx.x; gt < ntiles; gt += gridDim.x) {
+        if (tid == 0) {
+            stk_s = tile_stack[gt];
+            bs = stacks[stk_s];
+            sum_s = 0;
+            bad_s = 0;
+        }
+        __syncthreads();
+        const Geom &g = bs.g;
+        const TileInfo ti = tile_info(g, gt - bs.tile0);
+        const T *in = static_cast<const T *>(bs.in);
+        const uint32_t nunits = (ti.nblk + 7u) >> 3;
+        uint32_t sum = 0, bad = 0;
+        for (uint32_t u = warp; u < nunits; u += kWarps) {
+            const uint32_t b = u * 8u + jb;
+            const bool active = b < ti.nblk;
+            const unsigned long long rho = g.chunked ? ti.rho0 : ti.rho0 + (active ? b / g.bzb : 0u);
+            const uint32_t bz = g.chunked ? ti.c0 + b : (active ? b % g.bzb : 0u);
+            uint32_t nrows;
+            const unsigned long long e0 = (brow_start(g, rho, nrows) + r) * g.Z + 8ull * bz;
+            const uint32_t left = g.Z - 8u * bz, ncols = left < 8u ? left : 8u;
+            Row<T> A, B;
+#pragma unroll
+            for (int i = 0; i < Elem<T>::kWords; i++) A.w[i] = B.w[i] = 0;
+            for (uint32_t half = 0; half < 2u; half++) {
+                Row<T> &v = half ? B : A;
+                if (!active || r + 4u * half >= nrows) continue;
+                const T *p = in + e0 + 4ull * half * g.Z;
+                if (g.vec == 16) load_cols<T, 16>(p, ncols, v);
+                else if (sizeof(T) == 4 || g.vec == 4) load_cols<T, 4>(p, ncols, v);
+                else load_cols<T, 2>(p, ncols, v);
+            }
+            uint32_t rb;
+            const uint32_t h =
+                block_header<T, BINS == BINS_IDENT ? BINS_EQUAL : BINS, POOL, BINS == BINS_IDENT>(A, B, bs.c, rb);
+            if (active && r == 0) {
+                sum += (h & 0x1fu) << (3u - (h >> 7));  // rate planes of 8 bytes, or 4 when pooled
+                bad |= rb;
+            }
+        }
+        sum = __reduce_add_sync(0xffffffffu, sum);
+        bad = __reduce_or_sync(0xffffffffu, bad);
+        if (lane == 0) {
+            atomicAdd(&sum_s, sum);
+            atomicOr(&bad_s, bad);
+        }
+        __syncthreads();
+        if (tid == 0) {
+            atomicAdd(&payload[stk_s], (unsigned long long)sum_s);
+            if (bad_s) raise_error(ctl, DEV_ERR_RANGE);
+        }
+        __syncthreads();
+    }
+}
+
+template <typename T, int BINS>
+void launch_size_p(bool pool, unsigned grid, const BatchStack *stacks, const uint32_t *map, unsigned long long ntiles,
+                   unsigned long long *payload, LaunchCtl *ctl, cudaStream_t st)
+{
+    if (pool) size_kernel<T, BINS, true><<<grid, kThreads, 0, st>>>(stacks, map, ntiles, payload, ctl);
+    else size_kernel<T, BINS, false><<<grid, kThreads, 0, st>>>(stacks, map, ntiles, payload, ctl);
+}
+
+template <typename T>
+int stream_sizes_t(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, const uint32_t *bins,
+                   const float *pooling, uint64_t *stream_len, void *stream)
+{
+    if (!ws || !stream_len || (n && !stacks)) return LSCOMP_ERR_ARG;
+    if (n == 0) return LSCOMP_OK;
+    std::vector<Codec> codec;
+    int layout = 0;
+    bool pool = false;
+    if (!batch_codecs(bins, pooling, true, n, sizeof(T) == 4, codec, layout, pool)) return LSCOMP_ERR_ARG;
+    std::vector<Geom> geom;
+    std::vector<unsigned long long> tile0;
+    unsigned long long total = 0;
+    if (!batch_geoms(stacks, n, Elem<T>::kTileBlocks, geom, tile0, total)) return LSCOMP_ERR_ARG;
+    for (uint32_t s = 0; s < n; s++) {
+        if (!stacks[s].d_in || reinterpret_cast<uintptr_t>(stacks[s].d_in) % sizeof(T)) return LSCOMP_ERR_ARG;
+        geom[s].vec = (uint32_t)vec_class(stacks[s].d_in, stacks[s].z, sizeof(T));
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    std::lock_guard<std::mutex> lk(ws->mu);
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (prev != ws->device) cudaSetDevice(ws->device);
+    int r = batch_reserve(ws, n, total, st);
+    if (!r) r = ws_prepare(ws, 1, st);  // clears the control block
+    if (!r) {
+        for (uint32_t s = 0; s < n; s++) {
+            BatchStack &b = ws->h_stacks[s];
+            memset(&b, 0, sizeof(b));
+            b.g = geom[s];
+            b.c = codec[s];
+            b.in = stacks[s].d_in;
+            b.tile0 = tile0[s];
+        }
+        r = cuda_status(cudaMemcpyAsync(ws->d_stacks, ws->h_stacks, n * sizeof(BatchStack), cudaMemcpyHostToDevice, st));
+    }
+    if (!r) r = cuda_status(cudaMemsetAsync(ws->d_bsizes, 0, n * sizeof(unsigned long long), st));
+    if (!r) {
+        const uint32_t mgrid = n < 4096u ? n : 4096u;
+        tile_stack_kernel<<<mgrid, 256, 0, st>>>(ws->d_stacks, n, ws->d_tile_stack);
+        g_launches.fetch_add(1);
+        r = cuda_status(cudaGetLastError());
+    }
+    if (!r) {
+        unsigned long long grid = (unsigned long long)ws->sm_count * 8;
+        if (grid > total) grid = total;
+        const unsigned gr = (unsigned)grid;
+        switch (layout) {
+        case BINS_IDENT: launch_size_p<T, BINS_IDENT>(pool, gr, ws->d_stacks, ws->d_tile_stack, total, ws->d_bsizes, ws->ctl, st); break;
+        case BINS_EQUAL: launch_size_p<T, BINS_EQUAL>(pool, gr, ws->d_stacks, ws->d_tile_stack, total, ws->d_bsizes, ws->ctl, st); break;
+        case BINS_MONO: launch_size_p<T, BINS_MONO>(pool, gr, ws->d_stacks, ws->d_tile_stack, total, ws->d_bsizes, ws->ctl, st); break;
+        default: launch_size_p<T, BINS_GENERAL>(pool, gr, ws->d_stacks, ws->d_tile_stack, total, ws->d_bsizes, ws->ctl, st); break;
+        }
+        g_launches.fetch_add(1);
+        r = cuda_status(cudaGetLastError());
+    }
+    if (!r)
+        r = cuda_status(cudaMemcpyAsync(ws->h_bsizes, ws->d_bsizes, n * sizeof(unsigned long long),
+                                        cudaMemcpyDeviceToHost, st));
+    if (!r) r = read_ctl(ws, st);  // synchronises the stream
+    if (!r)
+        for (uint32_t s = 0; s < n; s++) stream_len[s] = geom[s].R + ws->h_bsizes[s];
+    if (prev != ws->device) cudaSetDevice(prev);
+    return r;
+}
+
 // ---------------------------------------------------------------- batch decompression
 // Many streams decoded by three launches: the stack of every tile, the
 // offsets kernel over every stack's segments, then one CTA per tile of every
@@ -240,10 +387,11 @@ int decompress_batch_t(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_
             return LSCOMP_ERR_ARG;
         if (q.cap < geom[s].nb) return LSCOMP_ERR_CAPACITY;
         const int v = vec_class(q.d_out, q.z, sizeof(T));
-        if (v < vec) vec = v;
+        if (sizeof(T) == 4 && v == 2) return LSCOMP_ERR_ARG;
+        geom[s].vec = (uint32_t)v;  // every stack is written with its own row access width
         seg0[s + 1] = seg0[s] + (geom[s].ntiles + kSegTiles - 1) / kSegTiles;
     }
-    if (sizeof(T) == 4 && vec == 2) return LSCOMP_ERR_ARG;
+    vec = sizeof(T) == 2 ? 2 : 4;
     if (total > 0x7fffffffull) return LSCOMP_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
     std::lock_guard<std::mutex> lk(ws->mu);
@@ -388,11 +536,9 @@ int plan_create_t(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, 
     bool pool = false;
     batch_codecs(bins, pooling, per_stack, n, sizeof(T) == 4, codec, layout, pool);
     const Codec &c = codec[0];
-    int vec = 16;
-    for (uint32_t s = 0; s < n; s++) {
-        const int v = vec_class(stacks[s].d_in, stacks[s].z, sizeof(T));
-        if (v < vec) vec = v;
-    }
+    // one stack: the single-stack kernel at the stack's row access width;
+    // several: the batch kernel, every stack at its own width (Geom::vec)
+    int vec = n == 1 ? vec_class(stacks[0].d_in, stacks[0].z, sizeof(T)) : (sizeof(T) == 2 ? 2 : 4);
     Geom g0;
     make_geom(stacks[0].x, stacks[0].y, stacks[0].z, Elem<T>::kTileBlocks, g0);
     TuneCfg cfg{-1, (uint32_t)Elem<T>::kTileBlocks};
@@ -427,6 +573,7 @@ int plan_create_t(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, 
         std::vector<BatchStack> h(n);
         for (uint32_t s = 0; s < n; s++) {
             h[s].g = geom[s];
+            h[s].g.vec = (uint32_t)vec_class(stacks[s].d_in, stacks[s].z, sizeof(T));
             h[s].c = codec[s];
             h[s].in = stacks[s].d_in;
             h[s].out = stacks[s].d_out;
@@ -543,6 +690,18 @@ int lscomp_compress_batch_ex_u32(lscomp_workspace *ws, const lscomp_stack *stack
                                  const float *pooling, uint64_t *stream_len, uint64_t *ref_size, void *stream)
 {
     return compress_batch_t<uint32_t>(ws, stacks, n, bins, pooling, true, stream_len, ref_size, stream);
+}
+
+int lscomp_stream_sizes_batch_u16(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, const uint32_t *bins,
+                                  const float *pooling, uint64_t *stream_len, void *stream)
+{
+    return stream_sizes_t<uint16_t>(ws, stacks, n, bins, pooling, stream_len, stream);
+}
+
+int lscomp_stream_sizes_batch_u32(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, const uint32_t *bins,
+                                  const float *pooling, uint64_t *stream_len, void *stream)
+{
+    return stream_sizes_t<uint32_t>(ws, stacks, n, bins, pooling, stream_len, stream);
 }
 
 int lscomp_decompress_batch_u16(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, const uint32_t *bins,

@@ -102,6 +102,7 @@ struct Geom {
     uint32_t G;                // block-rows per tile (whole-row tiles)
     uint32_t nc, W;            // chunks per block-row, chunk width (chunked tiles)
     uint32_t inv_bzb;          // ceil(65536 / bzb), exact b / bzb for b < 256 (whole-row tiles)
+    uint32_t vec;              // batch launches: widest row access of this stack (16, 4 or 2 bytes)
     unsigned long long byb_magic, nc_magic;  // ceil(2^64 / d) of byb and nc (0 for d = 1)
 };
 
@@ -251,6 +252,25 @@ __device__ __forceinline__ void load8(const uint8_t *p, Row<uint32_t> &v)
         const uint32_t *q = reinterpret_cast<const uint32_t *>(p);
 #pragma unroll
         for (int i = 0; i < 8; i++) v.w[i] = q[i];
+    }
+}
+
+// The first ncols (1..8) values at p (global memory), the rest 0; nothing
+// past them is read.  Full rows are read VEC bytes at a time.
+template <typename T, int VEC = sizeof(T)>
+__device__ __forceinline__ void load_cols(const T *p, uint32_t ncols, Row<T> &v)
+{
+    if (ncols >= 8u) {
+        load8<VEC>(reinterpret_cast<const uint8_t *>(p), v);
+        return;
+    }
+#pragma unroll
+    for (int i = 0; i < Elem<T>::kWords; i++) v.w[i] = 0;
+#pragma unroll
+    for (uint32_t i = 0; i < 8u; i++) {
+        if (i >= ncols) break;
+        if constexpr (sizeof(T) == 2) v.w[i >> 1] |= (uint32_t)p[i] << (16u * (i & 1u));
+        else v.w[i] = p[i];
     }
 }
 
@@ -613,8 +633,11 @@ __device__ __forceinline__ uint32_t xpose4(uint32_t x, const XSel &s)
 // ---------------------------------------------------------------- shared state
 // Encoder CTA: GRP x WPG compute warps in independent groups, one producer
 // warp (tile claims and TMA loads) and kWriters writer warps (look-back and
-// write-out, alternate tiles), one CTA per SM.
-constexpr int kWriters = 1;                   // writer warps (look-back and write-out)
+// write-out), one CTA per SM.  Writer w serves compute group w (the groups
+// take alternate tiles, so do the writers): two look-backs and two
+// copy-outs are in flight per SM, which a single writer's ~1 us look-back
+// round trip per tile would otherwise bound.
+constexpr int kWriters = 2;                   // writer warps (look-back and write-out)
 template <int GRP, int WPG> struct EncShape {
     static constexpr int kCompute = GRP * WPG;
     static constexpr int kThreads = (kCompute + 1 + kWriters) * 32;
@@ -632,8 +655,13 @@ struct EncSmem {
     alignas(128) uint8_t st[kStStages][kStagingBytes];
     uint64_t in_full[kInStages];       // producer -> compute: input of entries k = s mod 2 kInStages landed
     uint64_t in_empty[kInStages];      // compute -> producer: input slot read
-    uint64_t st_full[kStStages];       // compute -> writer: payload packed
-    uint64_t st_empty[kStStages];      // writer -> compute: payload written out
+    // payload packed (compute -> writer) and written out (writer -> compute)
+    // for ring entry k, one barrier per k mod 2 kStStages: the two writers
+    // take alternate entries and run independently, so a wait on one
+    // barrier per slot could pass on the phase of the entry two uses back
+    // (see st_full_bar)
+    uint64_t st_full[2 * kStStages];
+    uint64_t st_empty[2 * kStStages];
     unsigned long long in_tile[kInStages];
     uint32_t in_mis[kInStages][8];     // byte misalignment of each range start (mod 16)
     unsigned long long st_tile[kStStages];
@@ -673,6 +701,25 @@ __device__ __forceinline__ uint64_t *entry_full(EncSmem &sm, uint32_t k)
 }
 
 __device__ __forceinline__ uint32_t entry_parity(uint32_t k) { return (k / (2 * kInStages)) & 1u; }
+
+// Payload ring entry k (slot k mod kStStages): its fill barrier, its release
+// barrier and the parity of their phase.  Entry k's slot is free once entry
+// k - kStStages is released.  With barriers per entry mod 2 kStStages the
+// phase before entry k's on either barrier is entry k - 2 kStStages's, and
+// that one is always complete when entry k is waited for: the writer of k
+// consumed it (same writer), and the group filling k - kStStages needed it
+// released.  So a parity wait cannot pass on a stale phase.
+__device__ __forceinline__ uint64_t *st_full_bar(EncSmem &sm, uint32_t k) { return &sm.st_full[k % (2 * kStStages)]; }
+__device__ __forceinline__ uint64_t *st_empty_bar(EncSmem &sm, uint32_t k) { return &sm.st_empty[k % (2 * kStStages)]; }
+__device__ __forceinline__ uint32_t st_parity(uint32_t k) { return (k / (2 * kStStages)) & 1u; }
+
+// Wait until payload ring entry k's slot is free (entry k - kStStages
+// written out); the first kStStages entries find their slots free.
+__device__ __forceinline__ bool st_slot_free(EncSmem &sm, uint32_t k, LaunchCtl *ctl)
+{
+    if (k < (uint32_t)kStStages) return true;
+    return mbar_wait(st_empty_bar(sm, k - kStStages), st_parity(k - kStStages), ctl);
+}
 
 // payload bytes of one tile at most (uint16: 256 blocks x 16 planes x 8
 // bytes; uint32: 128 blocks x 31 planes x 8 bytes)
@@ -879,6 +926,17 @@ __device__ __forceinline__ void load_rows(const SegLoc &L, bool active, uint32_t
     }
 }
 
+// load_rows with the row access width chosen at run time (batch launches,
+// whose stacks differ in width and alignment)
+template <typename T>
+__device__ __forceinline__ void load_rows_any(const SegLoc &L, bool active, uint32_t r, Row<T> &A, Row<T> &B,
+                                              uint32_t vec)
+{
+    if (vec == 16) load_rows<T, 16>(L, active, r, A, B);
+    else if (sizeof(T) == 4 || vec == 4) load_rows<T, 4>(L, active, r, A, B);
+    else load_rows<T, 2>(L, active, r, A, B);
+}
+
 // Named barrier of one compute group (id, thread count), with the AND of a
 // predicate over the group's threads.
 __device__ __forceinline__ bool group_bar_and(uint32_t id, uint32_t nthreads, bool pred)
@@ -1081,15 +1139,14 @@ __device__ __forceinline__ void enc_compute(const EncArgs<T> &a, EncSmem &sm)
     uint32_t *const off = sm.off[grp];
     for (uint32_t k = grp;; k += GRP) {
         const int i = (int)(k % kInStages), j = (int)(k % kStStages);
-        const uint32_t m = k / kStStages;
         bool ok = mbar_wait(entry_full(sm, k), entry_parity(k), a.ctl);
         if (!group_bar_and(barid, WPG * 32, ok)) break;
         const unsigned long long t = sm.in_tile[i];  // tile index inside its stack
         if (t == kMarker) {
             // end of this CTA's tiles: hand an end marker to the writer
-            if (gtid == 0 && mbar_wait(&sm.st_empty[j], (m & 1u) ^ 1u, a.ctl)) {
+            if (gtid == 0 && st_slot_free(sm, k, a.ctl)) {
                 sm.st_tile[j] = t;
-                mbar_arrive_cnt(&sm.st_full[j], WPG);
+                mbar_arrive_cnt(st_full_bar(sm, k), WPG);
             }
             break;
         }
@@ -1125,7 +1182,8 @@ __device__ __forceinline__ void enc_compute(const EncArgs<T> &a, EncSmem &sm)
                 const bool active = b < ti.nblk;
                 SegLoc L = seg_locate<T, true>(g, ti, sm.br_rel[i], sm.br_rows[i], stage, sm.in_mis[i], active ? b : 0, r);
                 Row<T> ra, rb_;
-                load_rows<T, VEC>(L, active, r, ra, rb_);
+                if constexpr (BATCH) load_rows_any<T>(L, active, r, ra, rb_, g.vec);
+                else load_rows<T, VEC>(L, active, r, ra, rb_);
                 if (!RELOAD) {
                     A[RELOAD ? 0 : q] = ra;
                     B[RELOAD ? 0 : q] = rb_;
@@ -1157,7 +1215,7 @@ __device__ __forceinline__ void enc_compute(const EncArgs<T> &a, EncSmem &sm)
         }
         for (uint32_t b = gtid; b < ti.nblk; b += WPG * 32) out[ti.k0 + b] = hdr[b];
         bool free_ok = true;
-        if (gtid == 0) free_ok = mbar_wait(&sm.st_empty[j], (m & 1u) ^ 1u, a.ctl);
+        if (gtid == 0) free_ok = st_slot_free(sm, k, a.ctl);
         if (!group_bar_and(barid, WPG * 32, free_ok)) break;
 
         // ---- pass B: pack from registers into the payload ring
@@ -1172,7 +1230,8 @@ __device__ __forceinline__ void enc_compute(const EncArgs<T> &a, EncSmem &sm)
                 if (RELOAD) {
                     SegLoc L = seg_locate<T, true>(g, ti, sm.br_rel[i], sm.br_rows[i], stage, sm.in_mis[i],
                                                    active ? b : 0, r);
-                    load_rows<T, VEC>(L, active, r, ra, rb_);
+                    if constexpr (BATCH) load_rows_any<T>(L, active, r, ra, rb_, g.vec);
+                    else load_rows<T, VEC>(L, active, r, ra, rb_);
                 } else {
                     ra = A[RELOAD ? 0 : q];
                     rb_ = B[RELOAD ? 0 : q];
@@ -1194,7 +1253,7 @@ __device__ __forceinline__ void enc_compute(const EncArgs<T> &a, EncSmem &sm)
             }
         }
         __syncwarp();
-        if (lane == 0) mbar_arrive(&sm.st_full[j]);
+        if (lane == 0) mbar_arrive(st_full_bar(sm, k));
     }
 }
 
@@ -1276,8 +1335,7 @@ __device__ __forceinline__ void enc_writer(const EncArgs<T> &a, EncSmem &sm, uin
     unsigned long long floor_incl = 0;  // and its inclusive prefix
     for (uint32_t k = w;; k += kWriters) {
         const int j = (int)(k % kStStages);
-        const uint32_t m = k / kStStages;
-        bool ok = mbar_wait(&sm.st_full[j], m & 1u, a.ctl);
+        bool ok = mbar_wait(st_full_bar(sm, k), st_parity(k), a.ctl);
         if (!__all_sync(0xffffffffu, ok)) break;
         const unsigned long long t = sm.st_tile[j];  // tile index inside its stack
         if (t == kMarker) break;
@@ -1333,7 +1391,7 @@ __device__ __forceinline__ void enc_writer(const EncArgs<T> &a, EncSmem &sm, uin
             if (lane < (uint32_t)(g.R - g.nb)) out[g.nb + lane] = 0;  // header pad
         }
         __syncwarp();
-        if (lane == 0) mbar_arrive(&sm.st_empty[j]);
+        if (lane == 0) mbar_arrive(st_empty_bar(sm, k));
     }
 }
 
@@ -1342,7 +1400,7 @@ __global__ void __launch_bounds__(EncShape<GRP, WPG>::kThreads, 1) enc_kernel(co
 {
     using S = EncShape<GRP, WPG>;
     static_assert(GRP <= kMaxGroups, "compute groups");
-    static_assert(kWriters == 1, "end markers are passed to a single writer warp");
+    static_assert(kWriters == GRP, "writer w takes the tiles (and the end marker) of compute group w");
     extern __shared__ __align__(128) uint8_t smem_raw[];
     EncSmem &sm = *reinterpret_cast<EncSmem *>(smem_raw);
     const uint32_t tid = threadIdx.x, warp = tid >> 5;
@@ -1352,7 +1410,7 @@ __global__ void __launch_bounds__(EncShape<GRP, WPG>::kThreads, 1) enc_kernel(co
             mbar_init(&sm.in_full2[s], 1);
             mbar_init(&sm.in_empty[s], WPG);
         }
-        for (int s = 0; s < kStStages; s++) {
+        for (int s = 0; s < 2 * kStStages; s++) {
             mbar_init(&sm.st_full[s], WPG);
             mbar_init(&sm.st_empty[s], 1);
         }
@@ -1589,9 +1647,18 @@ __device__ __forceinline__ void dec_values(uint32_t Y[][4], uint32_t h, bool act
     }
 }
 
+// store8 with the row access width chosen at run time (batch launches)
+template <typename T>
+__device__ __forceinline__ void store8_any(T *p, const Row<T> &v, uint32_t ncols, uint32_t vec)
+{
+    if (vec == 16) store8<16>(p, v, ncols);
+    else if (sizeof(T) == 4 || vec == 4) store8<4>(p, v, ncols);
+    else store8<2>(p, v, ncols);
+}
+
 // Values of one unit from its plane words (dec_values), stored to rows r
-// and r+4 of block b.
-template <typename T, int VEC>
+// and r+4 of block b (BATCH: with the stack's own row access width).
+template <typename T, int VEC, bool BATCH>
 __device__ __forceinline__ void dec_unit(const DecArgs<T> &a, const TileInfo &ti, const DecSmem &sm, uint32_t Y[][4],
                                          uint32_t h, uint32_t b, uint32_t r, unsigned long long ebase)
 {
@@ -1602,8 +1669,13 @@ __device__ __forceinline__ void dec_unit(const DecArgs<T> &a, const TileInfo &ti
     dec_values<T>(Y, h, active, r, a.c.bins[(h >> 5) & 3u], A, B);
     if (active) {
         T *rowA = a.out + ebase + L.growA;
-        if (r < L.nrows) store8<VEC>(rowA, A, L.ncols);
-        if (r + 4 < L.nrows) store8<VEC>(rowA + 4ull * g.Z, B, L.ncols);
+        if constexpr (BATCH) {
+            if (r < L.nrows) store8_any<T>(rowA, A, L.ncols, g.vec);
+            if (r + 4 < L.nrows) store8_any<T>(rowA + 4ull * g.Z, B, L.ncols, g.vec);
+        } else {
+            if (r < L.nrows) store8<VEC>(rowA, A, L.ncols);
+            if (r + 4 < L.nrows) store8<VEC>(rowA + 4ull * g.Z, B, L.ncols);
+        }
     }
 }
 
@@ -1741,7 +1813,7 @@ __global__ void __launch_bounds__(kThreads, LSC_DEC_CTAS) dec_kernel(const DecAr
         const uint32_t o = sm.off[active ? b : 0] + __shfl_sync(0xffffffffu, wpre, u >> 2);  // 4 units per warp's 32 blocks
         uint32_t Y[NG][4];
         dec_load<T>(pay + (active ? o : 0u), h, r, Y);
-        dec_unit<T, VEC>(a, ti, sm, Y, h, b, r, ebase);
+        dec_unit<T, VEC, BATCH>(a, ti, sm, Y, h, b, r, ebase);
     }
 }
 

@@ -73,24 +73,6 @@ __device__ bool device_codec(const uint4 qb, float p, bool wide, Codec &c)
     return ok;
 }
 
-// The first ncols (1..8) values at p, the rest 0; nothing past them is read.
-template <typename T>
-__device__ __forceinline__ void load_cols(const T *p, uint32_t ncols, Row<T> &v)
-{
-    if (ncols >= 8u) {
-        load8<sizeof(T)>(reinterpret_cast<const uint8_t *>(p), v);
-        return;
-    }
-#pragma unroll
-    for (int i = 0; i < Elem<T>::kWords; i++) v.w[i] = 0;
-#pragma unroll
-    for (uint32_t i = 0; i < 8u; i++) {
-        if (i >= ncols) break;
-        if constexpr (sizeof(T) == 2) v.w[i >> 1] |= (uint32_t)p[i] << (16u * (i & 1u));
-        else v.w[i] = p[i];
-    }
-}
-
 // Rows r and r+4 of block b (block index order, z fastest) from global
 // memory; values outside the stack are 0.
 template <typename T>

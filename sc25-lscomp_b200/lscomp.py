@@ -138,6 +138,8 @@ def load_library() -> ctypes.CDLL:
                                                                     pu64, pu64, vp]
         getattr(lib, f"lscomp_decompress_batch_{sfx}").argtypes = [vp, ctypes.POINTER(LscompStack), u32,
                                                                    ctypes.POINTER(u32), ctypes.POINTER(f32), vp]
+        getattr(lib, f"lscomp_stream_sizes_batch_{sfx}").argtypes = [vp, ctypes.POINTER(LscompStack), u32,
+                                                                     ctypes.POINTER(u32), ctypes.POINTER(f32), pu64, vp]
         getattr(lib, f"lscomp_plan_create_ex_{sfx}").argtypes = [vp, ctypes.POINTER(LscompStack), u32,
                                                                  ctypes.POINTER(u32), ctypes.POINTER(f32), vp,
                                                                  ctypes.POINTER(vp)]
@@ -280,6 +282,30 @@ def _per_stack_settings(items):
             bins[4 * i + k] = int(b[k])
         pool[i] = float(p)
     return bins, pool
+
+
+def stream_sizes_batch(ws: Workspace, items, stream=None):
+    """Exact stream lengths of many stacks without compressing them:
+    items = [(d_in, dims, d_out or None, bins, pooling), ...] (one element
+    type; d_out is not used).  Returns [stream_len, ...], the bytes
+    compress_batch_mixed / compress_into would write."""
+    lib = load_library()
+    n = len(items)
+    if n == 0:
+        return []
+    sfx = _suffix(items[0][0])
+    arr = (LscompStack * n)()
+    for i, it in enumerate(items):
+        if _suffix(it[0]) != sfx:
+            raise ValueError("a batch holds one element type")
+        x, y, z = (int(v) for v in it[1])
+        arr[i] = LscompStack(it[0].data_ptr(), x, y, z, None, 0)
+    bins, pool = _per_stack_settings(items)
+    sl = (ctypes.c_uint64 * n)()
+    st = getattr(lib, f"lscomp_stream_sizes_batch_{sfx}")(ws.handle, arr, n, bins, pool, sl,
+                                                          ctypes.c_void_p(_stream_handle(stream)))
+    _check(st, f"lscomp_stream_sizes_batch_{sfx}")
+    return [int(v) for v in sl]
 
 
 def compress_batch_mixed(ws: Workspace, items, stream=None):

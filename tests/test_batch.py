@@ -258,3 +258,31 @@ def test_decompress_batch_truncated(lz, ws):
     # the workspace still works
     lz.decompress_batch(ws, [(out, sl, dims, dec, *LOSSLESS)])
     assert torch.equal(dec, d_in)
+
+
+@pytest.mark.parametrize("wide", [False, True])
+def test_stream_sizes_match_compression(lz, ws, wide):
+    """lscomp_stream_sizes_batch_*: the exact bytes compression writes, per
+    stack and per setting, from a pass that writes no stream; a uint32
+    quotient needing 32 planes is refused as compression refuses it."""
+    rng = np.random.default_rng(21)
+    settings = SETTINGS + [GENERAL]
+    shapes = SHAPES + [(3, 130, 150), (2, 300, 210)]
+    view, eb = (np.int32, 4) if wide else (np.int16, 2)
+    items = []
+    for i, dims in enumerate(shapes):
+        a = stack32(dims, seed=500 + i) if wide else stack16(dims, seed=500 + i)
+        b, p = settings[int(rng.integers(0, len(settings)))]
+        d_in = torch.from_numpy(a.view(view).ravel()).cuda()
+        out = torch.zeros(lz.max_stream_bytes(dims, eb), dtype=torch.uint8, device="cuda")
+        items.append((d_in, dims, out, b, p))
+    sizes = lz.stream_sizes_batch(ws, items)
+    res = lz.compress_batch_mixed(ws, items)
+    assert sizes == [sl for sl, _ in res]
+    if wide:
+        a = np.zeros((1, 8, 8), dtype=np.uint32)
+        a[0, 0, 0] = 0xFFFFFFFF
+        d = torch.from_numpy(a.view(np.int32).ravel()).cuda()
+        with pytest.raises(lz.LscompError) as e:
+            lz.stream_sizes_batch(ws, items[:2] + [(d, (1, 8, 8), None, LOSSLESS[0], 1.0)])
+        assert e.value.status == 6

@@ -2,7 +2,7 @@
 kernel header, lsCOMP/include/cuLSZ_kernel.h:9-36), launched as a caller of
 that header launches them: one 32-thread CTA per 1024 blocks and three
 zeroed scratch arrays (tests/culsz_kernel_driver.cu, built here with nvcc
-against liblscomp.so).
+and linked with liblscomp_kernels.a, the static archive of these kernels).
 
 Streams must equal the oracle's byte for byte, the size read from
 cmpOffset[grid] must be payload + nb (also for one-CTA grids, where the
@@ -35,10 +35,12 @@ def kdrv(tmp_path_factory):
 
     lscomp.load_library()
     so = str(tmp_path_factory.mktemp("kdrv") / "libkdrv.so")
+    # linked with the static kernel archive, as a program built against the
+    # reference's static library links its kernels
     subprocess.run(["nvcc", "-std=c++17", "-O2", "-gencode", "arch=compute_100a,code=sm_100a", "-Xcompiler",
                     "-fPIC", "-shared", "-I", os.path.join(ROOT, "include"),
-                    os.path.join(ROOT, "tests", "culsz_kernel_driver.cu"), "-o", so, "-L", PKG, "-llscomp",
-                    "-Xlinker", f"-rpath={PKG}"], check=True)
+                    os.path.join(ROOT, "tests", "culsz_kernel_driver.cu"), os.path.join(PKG, "liblscomp_kernels.a"),
+                    "-o", so], check=True)
     lib = ctypes.CDLL(so)
     vp, u, f32 = ctypes.c_void_p, ctypes.c_uint, ctypes.c_float
     pint = ctypes.POINTER(ctypes.c_int)
