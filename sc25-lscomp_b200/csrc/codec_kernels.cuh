@@ -633,13 +633,13 @@ __device__ __forceinline__ uint32_t xpose4(uint32_t x, const XSel &s)
 // ---------------------------------------------------------------- shared state
 // Encoder CTA: GRP x WPG compute warps in independent groups, one producer
 // warp (tile claims and TMA loads) and kWriters writer warps (look-back and
-// write-out), one CTA per SM.  Writer w serves compute group w (the groups
-// take alternate tiles, so do the writers): two look-backs and two
-// copy-outs are in flight per SM, which a single writer's ~1 us look-back
-// round trip per tile would otherwise bound.
-constexpr int kWriters = 2;                   // writer warps (look-back and write-out)
+// write-out), one CTA per SM.  With groups of up to 8 warps there is one
+// writer per group (writer w takes group w's tiles: two look-backs and two
+// copy-outs in flight per SM); groups of 13 warps keep a single writer,
+// whose 896 threads already use the register file at 72 registers each.
 template <int GRP, int WPG> struct EncShape {
     static constexpr int kCompute = GRP * WPG;
+    static constexpr int kWriters = WPG > 8 ? 1 : GRP;
     static constexpr int kThreads = (kCompute + 1 + kWriters) * 32;
     static constexpr int kProducerWarp = kCompute;
     static constexpr int kWriterWarp0 = kCompute + 1;
@@ -1058,6 +1058,10 @@ __device__ __forceinline__ void block_pack(const Row<T> &A0, const Row<T> &B0, u
     const bool pool = (h & 0x80u) != 0;
     const uint32_t rate = h & 0x1fu;
     const uint32_t choice = (h >> 5) & 3u;
+    // the unit's largest rate (the same in every lane): a unit of rate-0
+    // blocks only (mostly-zero data) has no planes, so nothing is quantised
+    const uint32_t wrate = __reduce_max_sync(0xffffffffu, rate);
+    if (wrate == 0u) return;
     Row<T> A = A0, B = B0;
     if (__any_sync(0xffffffffu, active && pool)) {
         // pooled blocks: lane r=0 takes row pair (0,1), r=1 (4,5), r=2 (2,3),
@@ -1084,7 +1088,6 @@ __device__ __forceinline__ void block_pack(const Row<T> &A0, const Row<T> &B0, u
         quant(A, c, choice);
         quant(B, c, choice);
     }
-    const uint32_t wrate = __reduce_max_sync(0xffffffffu, rate);
 #pragma unroll
     for (uint32_t grp = 0; grp < (uint32_t)NG; grp++) {
         if (wrate <= 8u * grp) break;
@@ -1293,17 +1296,30 @@ __device__ __forceinline__ void enc_producer(const EncArgs<T> &a, EncSmem &sm)
     const uint32_t lane = threadIdx.x & 31;
     const unsigned long long ntiles = BATCH ? a.ntiles_all : a.g.ntiles;
     uint32_t k = 0, ends = 0;
-    unsigned long long next = 0;  // the next tile, claimed one tile ahead
-    if (lane == 0) next = atomicAdd(&a.ctl->ticket, 1ull);
+    // lane 0 holds the next three tickets, claimed in program order (so in
+    // increasing order): a claim's round trip (about a microsecond under
+    // load) is spread over three tiles instead of bounding the issue rate
+    // at one tile per round trip.  Tiles are still taken in claim order, so
+    // every tile a look-back waits for belongs to a running CTA.
+    unsigned long long q0 = 0, q1 = 0, q2 = 0;
+    if (lane == 0) {
+        q0 = atomicAdd(&a.ctl->ticket, 1ull);
+        q1 = atomicAdd(&a.ctl->ticket, 1ull);
+        q2 = atomicAdd(&a.ctl->ticket, 1ull);
+    }
     for (;; k++) {
         const int i = (int)(k % kInStages);
         const uint32_t n = k / kInStages;
         bool ok = mbar_wait(&sm.in_empty[i], (n & 1u) ^ 1u, a.ctl);
         if (!__all_sync(0xffffffffu, ok)) break;
-        unsigned long long t = __shfl_sync(0xffffffffu, next, 0);
+        unsigned long long t = __shfl_sync(0xffffffffu, q0, 0);
         const bool real = t < ntiles;
         if (real) {
-            if (lane == 0) next = atomicAdd(&a.ctl->ticket, 1ull);
+            if (lane == 0) {
+                q0 = q1;
+                q1 = q2;
+                q2 = atomicAdd(&a.ctl->ticket, 1ull);
+            }
         } else {
             t = kMarker;
         }
@@ -1323,17 +1339,17 @@ __device__ __forceinline__ void enc_producer(const EncArgs<T> &a, EncSmem &sm)
     if (lane == 0) sm.issued = k;
 }
 
-// Writer warp w: for the CTA's tiles k = w, w + kWriters, ..., the look-back
+// Writer warp w: for the CTA's tiles k = w, w + NWR, ..., the look-back
 // for the tile's stream offset (bounded below by this writer's previous
 // tile, whose inclusive prefix it published itself), publication of the
 // inclusive prefix, and the copy of the packed payload to the stream.
-template <typename T, bool BATCH>
+template <typename T, bool BATCH, int NWR>
 __device__ __forceinline__ void enc_writer(const EncArgs<T> &a, EncSmem &sm, uint32_t w)
 {
     const uint32_t lane = threadIdx.x & 31;
     long long floor = -1;               // this writer's previous tile
     unsigned long long floor_incl = 0;  // and its inclusive prefix
-    for (uint32_t k = w;; k += kWriters) {
+    for (uint32_t k = w;; k += NWR) {
         const int j = (int)(k % kStStages);
         bool ok = mbar_wait(st_full_bar(sm, k), st_parity(k), a.ctl);
         if (!__all_sync(0xffffffffu, ok)) break;
@@ -1400,7 +1416,9 @@ __global__ void __launch_bounds__(EncShape<GRP, WPG>::kThreads, 1) enc_kernel(co
 {
     using S = EncShape<GRP, WPG>;
     static_assert(GRP <= kMaxGroups, "compute groups");
-    static_assert(kWriters == GRP, "writer w takes the tiles (and the end marker) of compute group w");
+    // a single writer takes every entry and stops at the first end marker
+    // (no real tile follows one); several take one group's entries each
+    static_assert(S::kWriters == 1 || S::kWriters == GRP, "writer w takes the tiles and the end marker of group w");
     extern __shared__ __align__(128) uint8_t smem_raw[];
     EncSmem &sm = *reinterpret_cast<EncSmem *>(smem_raw);
     const uint32_t tid = threadIdx.x, warp = tid >> 5;
@@ -1423,7 +1441,7 @@ __global__ void __launch_bounds__(EncShape<GRP, WPG>::kThreads, 1) enc_kernel(co
     else if (warp == (uint32_t)S::kProducerWarp)
         enc_producer<T, GRP, BATCH>(a, sm);
     else
-        enc_writer<T, BATCH>(a, sm, warp - (uint32_t)S::kWriterWarp0);
+        enc_writer<T, BATCH, S::kWriters>(a, sm, warp - (uint32_t)S::kWriterWarp0);
     __syncthreads();
     // After an error a load may still be in flight into a slot nobody
     // consumed; the last fill of every slot must land before the CTA's
@@ -1604,6 +1622,11 @@ __device__ __forceinline__ void dec_values(uint32_t Y[][4], uint32_t h, bool act
     const bool even = (r & 1u) == 0;
     const bool pool = (h & 0x80u) != 0;
     const uint32_t wrate = __reduce_max_sync(0xffffffffu, h & 0x1fu);
+    if (wrate == 0u) {  // every block of the unit has rate 0: all values are 0
+#pragma unroll
+        for (int i = 0; i < NW; i++) A.w[i] = B.w[i] = 0;
+        return;
+    }
     const XSel xs = xsel(r);
     // plane bytes per byte group, back in row order: [grp][0/1] = lo/hi half
     // of row r (PA) and of row r+4 (PB); groups and halves above the unit's
