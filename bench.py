@@ -79,6 +79,9 @@ def parse():
     ap.add_argument("--serve-arena-gb", type=int, default=120,
                     help="device arena of the serving benchmark's server (its admission cap)")
     ap.add_argument("--batch-frames", type=int, default=64, help="largest frame count of a batch stack")
+    ap.add_argument("--ref-build", choices=["sm_100a", "default"], default=None,
+                    help="with --impl reference: time this one build of the reference (default: each in a process of "
+                         "its own, the faster reported)")
     ap.add_argument("--ref-cpu", action="store_true",
                     help="with --impl reference: the oracle on the host cores instead of the reference's CUDA build")
     ap.add_argument("--ref-step-seconds", type=float, default=1.5,
@@ -649,6 +652,17 @@ def main():
     rank, world, local = dist_init(args.gpus)
     import torch
 
+    if args.impl == "reference" and not (args.ref_cpu or args.ref_build or args.batch or args.serve):
+        # each reference build in a process of its own; rank 0 reports
+        if rank == 0:
+            print(json.dumps(reference_builds(args)), flush=True)
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
     if args.batch:
         torch.cuda.set_device(local)
         if rank == 0:
@@ -1009,23 +1023,53 @@ def bench_reference_cpu(args, dims, config):
             "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def reference_builds(args):
+    """Both builds of the reference's CUDA sources, each timed in a process of
+    its own (one reference library per process: two in one process measured
+    the second one several times slower): nvcc -O3 for sm_100a, and nvcc's
+    default target as the reference's own CMake builds it (PTX compiled by
+    the driver on B200).  Returns the line of the faster build, with both
+    builds' step times."""
+    lines = {}
+    for b in ("sm_100a", "default"):
+        cmd = [sys.executable, os.path.abspath(__file__), "--impl", "reference", "--ref-build", b, "--steps",
+               str(args.steps), "--warmup", str(args.warmup), "--e2e-steps", str(args.e2e_steps), "--kind", args.kind]
+        if args.dims:
+            cmd += ["--dims", args.dims]
+        if args.no_per_config:
+            cmd.append("--no-per-config")
+        env = {k: v for k, v in os.environ.items()
+               if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK", "LOCAL_WORLD_SIZE", "GROUP_RANK", "MASTER_ADDR",
+                            "MASTER_PORT", "TORCHELASTIC_RUN_ID")}
+        r = subprocess.run(cmd, capture_output=True, text=True, env=env)
+        for ln in reversed(r.stdout.splitlines()):
+            if ln.startswith("{"):
+                d = json.loads(ln)
+                if "unavailable" not in d:
+                    lines[b] = d
+                break
+    if not lines:
+        return {"impl": "reference", "unavailable": "reference build missing or failed (oracle/_ref)"}
+    best = min(lines, key=lambda b: lines[b]["ms_per_step"])
+    out = lines[best]
+    out["ms_per_step_by_build"] = {b: d["ms_per_step"] for b, d in lines.items()}
+    return out
+
+
 def bench_reference_gpu(args, dims, dev, d_in, d_cmp, d_dec, nbytes, config, h):
-    """Both builds of the reference's CUDA sources are timed on the same
-    steps -- nvcc -O3 for sm_100a, and nvcc's default target as the
-    reference's own CMake builds it (PTX compiled by the driver on B200) --
-    and the faster one is the arm's value, e2e and per-config figures."""
+    """One build of the reference's CUDA sources (--ref-build: sm_100a, or
+    the default-target PTX build) through its host API on the same stack and
+    steps: value with the stack resident in HBM, e2e through host buffers,
+    and the other plain stacks (per_config)."""
     import torch
 
     try:
         from oracle import REF_LIB, REF_LIB_DEFAULT, RefLib
 
-        refs = [("sm_100a", RefLib(REF_LIB))]
+        label = "sm_100a" if args.ref_build == "sm_100a" else "default arch (PTX JIT)"
+        ref = RefLib(REF_LIB if args.ref_build == "sm_100a" else REF_LIB_DEFAULT)
     except Exception as e:  # the reference build is not present
         return {"impl": "reference", "unavailable": f"reference build missing: {e}"}
-    try:
-        refs.append(("default arch (PTX JIT)", RefLib(REF_LIB_DEFAULT)))
-    except Exception:
-        pass
     stream = torch.cuda.current_stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
@@ -1054,18 +1098,7 @@ def bench_reference_gpu(args, dims, dev, d_in, d_cmp, d_dec, nbytes, config, h):
         clk = clocks.stop() if clocks else None
         return e0.elapsed_time(e1) / steps, sizes, clk
 
-    builds = {}
-    for label, ref in refs[1:]:
-        ms_b, _, _ = run(ref, max(1, args.steps // 2))
-        builds[label] = round(ms_b, 4)
-    ms, sizes, clk = run(refs[0][1], args.steps, ClockSampler(torch.cuda.current_device()))
-    builds[refs[0][0]] = round(ms, 4)
-    label = min(builds, key=builds.get)
-    ref = dict(refs)[label]
-    if label != refs[0][0]:
-        # the faster build takes the timed steps again, clocks sampled
-        ms, sizes, clk = run(ref, args.steps, ClockSampler(torch.cuda.current_device()))
-        builds[label] = round(ms, 4)
+    ms, sizes, clk = run(ref, args.steps, ClockSampler(torch.cuda.current_device()))
     value = 4 * nbytes / (ms / 1e3) / 1e9
     e2e = None
     if args.e2e_steps > 0:
@@ -1110,10 +1143,11 @@ def bench_reference_gpu(args, dims, dev, d_in, d_cmp, d_dec, nbytes, config, h):
             "value": round(value, 2), "unit": "GB/s", "n_gpus": 1, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": round(ms, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": data_note(args.kind),
-            "config": config, "clocks": clk, "build": label, "ms_per_step_by_build": builds,
+            "config": config, "clocks": clk, "build": label,
             "cpu_baseline": {"value": round(value, 2), "unit": "GB/s", "cores": 1, "kind": "reference",
-                             "sample": f"the reference's CUDA sources ({label} build, the faster of the two) "
-                                       "through its host API on the full stack; the reference has no CPU "
+                             "sample": f"the reference's CUDA sources ({label} build; without --ref-build the faster "
+                                       "of its two builds is reported) through its host API on the full stack; "
+                                       "the reference has no CPU "
                                        "implementation (bench.py --impl reference --ref-cpu times the C/OpenMP "
                                        "oracle on the host cores)"},
             "e2e": e2e, "per_config": per_config}
