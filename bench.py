@@ -532,7 +532,7 @@ def bench_batch(args, local):
 def tuned_summary(lscomp, kinds=("compress", "batch", "decompress")):
     """The tuner's choices so far: key -> chosen shape/tile size and the
     candidates' measured ms per call."""
-    shapes = {-1: "rule", 0: "2x8", 1: "2x7", 2: "2x13"}
+    shapes = {-1: "rule", 0: "2x8", 1: "2x7", 2: "2x13", 3: "2pass"}
     out = []
     for e in lscomp.tune_table():
         if e["kind"] not in kinds:
@@ -643,7 +643,7 @@ def bench_serve(args, local):
                                              "1024x1024 (XPCS-like) or 1813x1558 (CSSI-like) uint16 frames; 70/30 "
                                              "compress/decompress; 60/40 lossless/lossy", "arena_bytes": arena,
                                  "duration_s_per_rate": args.serve_seconds,
-                                 "copy_threads_per_direction": int(os.environ.get("LSCOMP_SERVER_COPY_THREADS", 4))}}))
+                                 "copy_threads_per_direction": int(os.environ.get("LSCOMP_SERVER_COPY_THREADS", 8))}}))
 
 
 def main():

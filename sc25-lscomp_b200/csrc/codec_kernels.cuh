@@ -123,6 +123,7 @@ struct EncArgs {
     unsigned long long cap;
     LaunchCtl *ctl;
     unsigned long long *state;
+    unsigned long long *tile_off;   // two-pass encoder: per-tile payload offsets (ntiles + 1)
     uint32_t epoch;
     unsigned long long *sizes_out;  // optional device copy of {stream_len, payload}
     // batch launches: the stacks, the stack of every tile (tiles of all
@@ -1837,6 +1838,177 @@ __global__ void __launch_bounds__(kThreads, LSC_DEC_CTAS) dec_kernel(const DecAr
         uint32_t Y[NG][4];
         dec_load<T>(pay + (active ? o : 0u), h, r, Y);
         dec_unit<T, VEC, BATCH>(a, ti, sm, Y, h, b, r, ebase);
+    }
+}
+
+// ---------------------------------------------------------------- two-pass encoder
+// The same stream from three launches with no wait between CTAs: the
+// statistics kernel writes every block's header byte, dec_offsets_kernel
+// turns the header bytes into per-tile payload offsets (as for decoding),
+// and the pack kernel quantises and packs each tile into shared memory and
+// copies it to its offset.  The input is read twice, but each kernel is a
+// plain one-CTA-per-tile kernel: several CTAs per SM hide one another's
+// latencies, where the persistent single-pass encoder keeps one CTA per SM
+// busy with a long chain of per-tile hand-offs (ring barriers, look-back,
+// write-out).  Which of the two runs is the tuner's choice per shape.
+
+// The block-row table of tile ti (as dec_kernel builds it): element offset
+// of each block-row from the tile's first row and its row count; returns
+// the tile's first row.
+template <typename T>
+__device__ __forceinline__ unsigned long long tile_rows(const Geom &g, const TileInfo &ti, uint32_t *br_rel,
+                                                        uint8_t *br_rows)
+{
+    const uint32_t tid = threadIdx.x;
+    uint32_t n0;
+    const unsigned long long row0 = brow_start(g, ti.rho0, n0);
+    if (!g.chunked) {
+        if (tid < ti.nbr) {
+            uint32_t nrows;
+            const unsigned long long rs = brow_start(g, ti.rho0 + tid, nrows);
+            br_rel[tid] = (uint32_t)((rs - row0) * g.Z);
+            br_rows[tid] = (uint8_t)nrows;
+        }
+    } else if (tid == 0) {
+        br_rows[0] = (uint8_t)n0;
+    }
+    return row0;
+}
+
+// Rows r and r+4 of tile block b straight from global memory (VEC-byte
+// accesses; a block's columns past the stack's edge are neither read nor
+// kept: zeros, lsCOMP/src/cuLSZ_kernel.cu:877-896).
+template <typename T, int VEC>
+__device__ __forceinline__ void tile_block_rows(const T *in, const Geom &g, const TileInfo &ti, const uint32_t *br_rel,
+                                                const uint8_t *br_rows, unsigned long long ebase, uint32_t b,
+                                                bool active, uint32_t r, Row<T> &A, Row<T> &B)
+{
+    const SegLoc L = seg_locate<T, false>(g, ti, br_rel, br_rows, nullptr, nullptr, active ? b : 0u, r);
+#pragma unroll
+    for (int i = 0; i < Elem<T>::kWords; i++) A.w[i] = B.w[i] = 0;
+    const T *p = in + ebase + L.growA;
+    if (active && r < L.nrows) load_cols<T, VEC>(p, L.ncols, A);
+    if (active && r + 4 < L.nrows) load_cols<T, VEC>(p + 4ull * g.Z, L.ncols, B);
+}
+
+// Pass 1: the header byte of every block of tile blockIdx.x
+// (lsCOMP/src/cuLSZ_kernel.cu:898-957), written to the stream.
+template <typename T, int VEC, int BINS, bool POOL>
+__global__ void __launch_bounds__(kThreads, 6) enc_stats_kernel(const EncArgs<T> a)
+{
+    __shared__ uint32_t br_rel[kMaxTileBlocks];
+    __shared__ uint8_t br_rows[kMaxTileBlocks];
+    __shared__ uint8_t hdr[kMaxTileBlocks];
+    __shared__ uint32_t bad_s;
+    const Geom &g = a.g;
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, jb = lane & 7, r = lane >> 3;
+    const unsigned long long t = blockIdx.x;
+    const TileInfo ti = tile_info(g, t);
+    const unsigned long long ebase = tile_rows<T>(g, ti, br_rel, br_rows) * g.Z;
+    if (tid == 0) bad_s = 0;
+    __syncthreads();
+    const uint32_t nunits = (ti.nblk + 7) >> 3;
+    uint32_t bad = 0;
+    for (uint32_t u = warp; u < nunits; u += kWarps) {
+        const uint32_t b = u * 8 + jb;
+        const bool active = b < ti.nblk;
+        Row<T> A, B;
+        tile_block_rows<T, VEC>(a.in, g, ti, br_rel, br_rows, ebase, b, active, r, A, B);
+        uint32_t rb;
+        const uint32_t h =
+            block_header<T, BINS == BINS_IDENT ? BINS_EQUAL : BINS, POOL, BINS == BINS_IDENT>(A, B, a.c, rb);
+        if (active && r == 0) {
+            hdr[b] = (uint8_t)h;
+            bad |= rb;
+        }
+    }
+    if (__any_sync(0xffffffffu, bad != 0) && lane == 0) atomicOr(&bad_s, 1u);
+    __syncthreads();
+    if (tid < ti.nblk) a.out[ti.k0 + tid] = hdr[tid];
+    // a uint32 quotient >= 2^31 needs 32 planes, which the 5-bit rate field
+    // cannot hold
+    if (tid == 0 && bad_s) raise_error(a.ctl, DEV_ERR_RANGE);
+}
+
+// Pass 2: tile blockIdx.x's bit planes (lsCOMP/src/cuLSZ_kernel.cu:1100-1276)
+// packed in shared memory at the in-tile offsets its header bytes give,
+// then copied to the stream at R + tile_off[t] with consecutive 4-byte
+// words per thread; the last tile writes the totals and the header pad.
+template <typename T, int VEC, int BINS, bool POOL>
+__global__ void __launch_bounds__(kThreads, 4) enc_pack_kernel(const EncArgs<T> a)
+{
+    __shared__ alignas(16) uint8_t st[kStagingBytes];
+    __shared__ uint32_t off[kMaxTileBlocks];
+    __shared__ uint8_t hdr[kMaxTileBlocks];
+    __shared__ uint32_t wsum[kWarps];
+    __shared__ uint32_t br_rel[kMaxTileBlocks];
+    __shared__ uint8_t br_rows[kMaxTileBlocks];
+    const Geom &g = a.g;
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, jb = lane & 7, r = lane >> 3;
+    if (aborted(a.ctl)) return;  // pass 1 or the offsets failed: the stream is not written
+    const unsigned long long t = blockIdx.x;
+    const TileInfo ti = tile_info(g, t);
+    const unsigned long long ebase = tile_rows<T>(g, ti, br_rel, br_rows) * g.Z;
+    {
+        // block tid: header byte, size, offset inside the warp's 32 blocks
+        const uint32_t h = tid < ti.nblk ? a.out[ti.k0 + tid] : 0u;
+        const uint32_t sz = (h & 0x1fu) << (3u - (h >> 7));
+        uint32_t inc = sz;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t x = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= (uint32_t)o) inc += x;
+        }
+        hdr[tid] = (uint8_t)h;
+        off[tid] = inc - sz;
+        if (lane == 31) wsum[warp] = inc;
+    }
+    __syncthreads();
+    uint32_t wpre;  // lane w < kWarps: payload bytes of warps 0 .. w-1
+    {
+        const uint32_t v = lane < (uint32_t)kWarps ? wsum[lane] : 0u;
+        uint32_t inc = v;
+#pragma unroll
+        for (int o = 1; o < kWarps; o <<= 1) {
+            const uint32_t x = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= (uint32_t)o) inc += x;
+        }
+        wpre = inc - v;
+    }
+    const uint32_t agg = __shfl_sync(0xffffffffu, wpre, kWarps - 1) + wsum[kWarps - 1];
+    const unsigned long long base = a.tile_off[t];
+    if (g.R + base + agg > a.cap) {  // the same in every thread
+        if (tid == 0) raise_error(a.ctl, DEV_ERR_CAPACITY);
+        return;
+    }
+    const XSel xs = xsel(r);
+    const uint32_t nunits = (ti.nblk + 7) >> 3;
+    for (uint32_t u = warp; u < nunits; u += kWarps) {
+        const uint32_t b = u * 8 + jb;
+        const bool active = b < ti.nblk;
+        Row<T> A, B;
+        tile_block_rows<T, VEC>(a.in, g, ti, br_rel, br_rows, ebase, b, active, r, A, B);
+        const uint32_t h = active ? hdr[b] : 0u;
+        const uint32_t o = off[active ? b : 0] + __shfl_sync(0xffffffffu, wpre, u >> 2);  // 4 units per 32 blocks
+        block_pack<T, BINS == BINS_IDENT>(A, B, h, active, r, xs, a.c, st + (active ? o : 0u));
+    }
+    __syncthreads();
+    {
+        const uint32_t *s32 = reinterpret_cast<const uint32_t *>(st);
+        uint32_t *d32 = reinterpret_cast<uint32_t *>(a.out + g.R + base);
+        const uint32_t nw = agg / 4u;
+        for (uint32_t w = tid; w < nw; w += kThreads) d32[w] = s32[w];
+    }
+    if (t == g.ntiles - 1) {
+        if (tid == 0) {
+            a.ctl->total = base + agg;
+            a.ctl->stream_len = g.R + base + agg;
+            if (a.sizes_out) {
+                a.sizes_out[0] = g.R + base + agg;
+                a.sizes_out[1] = base + agg;
+            }
+        }
+        if (tid < (uint32_t)(g.R - g.nb)) a.out[g.nb + tid] = 0;  // header pad
     }
 }
 

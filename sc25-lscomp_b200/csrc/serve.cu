@@ -187,7 +187,7 @@ class CopyPool {
 unsigned copy_threads()
 {
     const char *e = getenv("LSCOMP_SERVER_COPY_THREADS");
-    const int n = e ? atoi(e) : 4;
+    const int n = e ? atoi(e) : 8;
     return n < 0 ? 0u : (n > 32 ? 32u : (unsigned)n);
 }
 
