@@ -264,7 +264,10 @@ inline int launch_enc_2p(const EncArgs<T> &a, int sm_count, cudaStream_t st)
     g_launches.fetch_add(1);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_status(e);
-    enc_pack_kernel<T, VEC, BINS, POOL><<<(unsigned)a.g.ntiles, kThreads, 0, st>>>(a);
+    auto pack = enc_pack_kernel<T, VEC, BINS, POOL>;
+    const size_t psmem = sizeof(PackSmem);
+    cudaFuncSetAttribute(pack, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem);
+    pack<<<(unsigned)a.g.ntiles, kThreads, psmem, st>>>(a);
     g_launches.fetch_add(1);
     return cuda_status(cudaGetLastError());
 }

@@ -786,21 +786,24 @@ __device__ __forceinline__ unsigned long long tile_prefix(unsigned long long *st
 }
 
 // ---------------------------------------------------------------- encoder
-// Producer warp, all lanes: the block-row table, range bookkeeping and TMA
-// issue of tile t into input slot s; the copies complete on `full`.  The
-// block-row starts of the tile are computed one per lane, so the warp's
-// dependent chain is that of a single block-row.
+// Where one tile's input lands in shared memory: the staging bytes, the
+// byte misalignment of each copied range (mod 16), and the block-row table
+// (element offset of each block-row from the tile's first row, its rows).
+struct TileStage {
+    uint8_t *in;
+    uint32_t *mis;
+    uint32_t *br_rel;
+    uint8_t *br_rows;
+};
+
+// One warp, all lanes: the block-row table, range bookkeeping and TMA issue
+// of tile t into ts; the copies complete on `full`.  The block-row starts
+// of the tile are computed one per lane, so the warp's dependent chain is
+// that of a single block-row.
 template <typename T>
-__device__ void enc_issue(const Geom &g, const T *in, EncSmem &sm, int s, unsigned long long t, uint64_t *full,
-                          uint32_t lane)
+__device__ void issue_tile(const Geom &g, const T *in, const TileStage &ts, unsigned long long t, uint64_t *full,
+                           uint32_t lane)
 {
-    if (t == kMarker) {
-        if (lane == 0) {
-            sm.in_tile[s] = t;
-            mbar_arrive(full);
-        }
-        return;
-    }
     constexpr uint32_t ES = sizeof(T);
     const TileInfo ti = tile_info(g, t);
     // ranges: whole-row tiles -> 1 contiguous range; chunked -> one per row.
@@ -819,8 +822,8 @@ __device__ void enc_issue(const Geom &g, const T *in, EncSmem &sm, int s, unsign
             }
             if (q0 == 0) r0 = __shfl_sync(0xffffffffu, rs, 0);
             if (q < ti.nbr) {
-                sm.br_rel[s][q] = (uint32_t)((rs - r0) * g.Z);
-                sm.br_rows[s][q] = (uint8_t)nrows;
+                ts.br_rel[q] = (uint32_t)((rs - r0) * g.Z);
+                ts.br_rows[q] = (uint8_t)nrows;
             }
             const uint32_t last = ti.nbr - q0;  // lane holding the end row in this pass
             if (last < 32u) rend = __shfl_sync(0xffffffffu, rs, last);
@@ -831,7 +834,7 @@ __device__ void enc_issue(const Geom &g, const T *in, EncSmem &sm, int s, unsign
     } else {
         uint32_t rows;
         const unsigned long long r0 = brow_start(g, ti.rho0, rows);
-        if (lane == 0) sm.br_rows[s][0] = (uint8_t)rows;
+        if (lane == 0) ts.br_rows[0] = (uint8_t)rows;
         const uint32_t col0 = 8u * ti.c0;
         uint32_t col1 = 8u * (ti.c0 + ti.nblk);
         if (col1 > g.Z) col1 = g.Z;
@@ -846,11 +849,11 @@ __device__ void enc_issue(const Geom &g, const T *in, EncSmem &sm, int s, unsign
     uintptr_t cs = 0, ce = 0;
     uint8_t *dst = nullptr;
     if (lane < nr) {
-        uint8_t *sb = sm.in[s] + (g.chunked ? lane * kChunkPitch : 0u);
+        uint8_t *sb = ts.in + (g.chunked ? lane * kChunkPitch : 0u);
         const uintptr_t ga = base + ES * es;
         const uintptr_t ge = ga + ES * ne;
         const uintptr_t gs = ga & ~(uintptr_t)15;
-        sm.in_mis[s][lane] = (uint32_t)(ga & 15);
+        ts.mis[lane] = (uint32_t)(ga & 15);
         cs = gs > A0 ? gs : A0;
         ce = (ge + 15) & ~(uintptr_t)15;
         if (ce > A1) ce = A1;
@@ -863,13 +866,25 @@ __device__ void enc_issue(const Geom &g, const T *in, EncSmem &sm, int s, unsign
         for (uintptr_t p = (ga > A1 ? ga : A1); p < ge; p += ES)
             *reinterpret_cast<T *>(sb + (p - gs)) = *reinterpret_cast<const T *>(p);
     }
-    if (lane == 0) sm.in_tile[s] = t;
     fence_proxy_async_smem();
     tx = __reduce_add_sync(0xffffffffu, tx);
     __syncwarp();
     if (lane == 0) mbar_arrive_expect_tx(full, tx);
     __syncwarp();
     if (lane < nr && ce > cs) bulk_g2s(dst, reinterpret_cast<const void *>(cs), (uint32_t)(ce - cs), full);
+}
+
+// Producer warp, all lanes: tile t (or the end marker) into input slot s.
+template <typename T>
+__device__ void enc_issue(const Geom &g, const T *in, EncSmem &sm, int s, unsigned long long t, uint64_t *full,
+                          uint32_t lane)
+{
+    if (lane == 0) sm.in_tile[s] = t;
+    if (t == kMarker) {
+        if (lane == 0) mbar_arrive(full);
+        return;
+    }
+    issue_tile<T>(g, in, TileStage{sm.in[s], sm.in_mis[s], sm.br_rel[s], sm.br_rows[s]}, t, full, lane);
 }
 
 // Where a lane's two row segments (rows r and r+4 of tile-local block b)
@@ -1852,43 +1867,21 @@ __global__ void __launch_bounds__(kThreads, LSC_DEC_CTAS) dec_kernel(const DecAr
 // busy with a long chain of per-tile hand-offs (ring barriers, look-back,
 // write-out).  Which of the two runs is the tuner's choice per shape.
 
-// The block-row table of tile ti (as dec_kernel builds it): element offset
-// of each block-row from the tile's first row and its row count; returns
-// the tile's first row.
+// Tile blockIdx.x's input into shared memory: warp 0 builds the block-row
+// table and issues the TMA bulk copies (issue_tile, as the persistent
+// encoder's producer does), every thread waits for them to land (bounded).
+// false if they did not land in time.
 template <typename T>
-__device__ __forceinline__ unsigned long long tile_rows(const Geom &g, const TileInfo &ti, uint32_t *br_rel,
-                                                        uint8_t *br_rows)
+__device__ __forceinline__ bool tile_in(const EncArgs<T> &a, const TileStage &ts, uint64_t *full)
 {
     const uint32_t tid = threadIdx.x;
-    uint32_t n0;
-    const unsigned long long row0 = brow_start(g, ti.rho0, n0);
-    if (!g.chunked) {
-        if (tid < ti.nbr) {
-            uint32_t nrows;
-            const unsigned long long rs = brow_start(g, ti.rho0 + tid, nrows);
-            br_rel[tid] = (uint32_t)((rs - row0) * g.Z);
-            br_rows[tid] = (uint8_t)nrows;
-        }
-    } else if (tid == 0) {
-        br_rows[0] = (uint8_t)n0;
+    if (tid == 0) {
+        mbar_init(full, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    return row0;
-}
-
-// Rows r and r+4 of tile block b straight from global memory (VEC-byte
-// accesses; a block's columns past the stack's edge are neither read nor
-// kept: zeros, lsCOMP/src/cuLSZ_kernel.cu:877-896).
-template <typename T, int VEC>
-__device__ __forceinline__ void tile_block_rows(const T *in, const Geom &g, const TileInfo &ti, const uint32_t *br_rel,
-                                                const uint8_t *br_rows, unsigned long long ebase, uint32_t b,
-                                                bool active, uint32_t r, Row<T> &A, Row<T> &B)
-{
-    const SegLoc L = seg_locate<T, false>(g, ti, br_rel, br_rows, nullptr, nullptr, active ? b : 0u, r);
-#pragma unroll
-    for (int i = 0; i < Elem<T>::kWords; i++) A.w[i] = B.w[i] = 0;
-    const T *p = in + ebase + L.growA;
-    if (active && r < L.nrows) load_cols<T, VEC>(p, L.ncols, A);
-    if (active && r + 4 < L.nrows) load_cols<T, VEC>(p + 4ull * g.Z, L.ncols, B);
+    __syncthreads();
+    if (tid < 32) issue_tile<T>(a.g, a.in, ts, blockIdx.x, full, tid);
+    return __syncthreads_and(mbar_wait_landed(full, 0)) != 0;
 }
 
 // Pass 1: the header byte of every block of tile blockIdx.x
@@ -1896,24 +1889,29 @@ __device__ __forceinline__ void tile_block_rows(const T *in, const Geom &g, cons
 template <typename T, int VEC, int BINS, bool POOL>
 __global__ void __launch_bounds__(kThreads, 6) enc_stats_kernel(const EncArgs<T> a)
 {
+    __shared__ alignas(128) uint8_t in_s[kStageBytes];
+    __shared__ uint32_t mis_s[8];
     __shared__ uint32_t br_rel[kMaxTileBlocks];
     __shared__ uint8_t br_rows[kMaxTileBlocks];
     __shared__ uint8_t hdr[kMaxTileBlocks];
+    __shared__ uint64_t full;
     __shared__ uint32_t bad_s;
     const Geom &g = a.g;
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, jb = lane & 7, r = lane >> 3;
-    const unsigned long long t = blockIdx.x;
-    const TileInfo ti = tile_info(g, t);
-    const unsigned long long ebase = tile_rows<T>(g, ti, br_rel, br_rows) * g.Z;
     if (tid == 0) bad_s = 0;
-    __syncthreads();
+    if (!tile_in<T>(a, TileStage{in_s, mis_s, br_rel, br_rows}, &full)) {
+        if (tid == 0) raise_error(a.ctl, DEV_ERR_TIMEOUT);
+        return;
+    }
+    const TileInfo ti = tile_info(g, blockIdx.x);
     const uint32_t nunits = (ti.nblk + 7) >> 3;
     uint32_t bad = 0;
     for (uint32_t u = warp; u < nunits; u += kWarps) {
         const uint32_t b = u * 8 + jb;
         const bool active = b < ti.nblk;
+        const SegLoc L = seg_locate<T, true>(g, ti, br_rel, br_rows, in_s, mis_s, active ? b : 0u, r);
         Row<T> A, B;
-        tile_block_rows<T, VEC>(a.in, g, ti, br_rel, br_rows, ebase, b, active, r, A, B);
+        load_rows<T, VEC>(L, active, r, A, B);
         uint32_t rb;
         const uint32_t h =
             block_header<T, BINS == BINS_IDENT ? BINS_EQUAL : BINS, POOL, BINS == BINS_IDENT>(A, B, a.c, rb);
@@ -1930,27 +1928,36 @@ __global__ void __launch_bounds__(kThreads, 6) enc_stats_kernel(const EncArgs<T>
     if (tid == 0 && bad_s) raise_error(a.ctl, DEV_ERR_RANGE);
 }
 
+// Shared memory of the packing kernel (dynamic: more than 48 KB).
+struct PackSmem {
+    alignas(128) uint8_t in[kStageBytes];
+    alignas(16) uint8_t st[kStagingBytes];
+    uint32_t mis[8];
+    uint32_t br_rel[kMaxTileBlocks];
+    uint8_t br_rows[kMaxTileBlocks];
+    uint32_t off[kMaxTileBlocks];
+    uint8_t hdr[kMaxTileBlocks];
+    uint32_t wsum[kWarps];
+    uint64_t full;
+};
+
 // Pass 2: tile blockIdx.x's bit planes (lsCOMP/src/cuLSZ_kernel.cu:1100-1276)
 // packed in shared memory at the in-tile offsets its header bytes give,
 // then copied to the stream at R + tile_off[t] with consecutive 4-byte
 // words per thread; the last tile writes the totals and the header pad.
 template <typename T, int VEC, int BINS, bool POOL>
-__global__ void __launch_bounds__(kThreads, 4) enc_pack_kernel(const EncArgs<T> a)
+__global__ void __launch_bounds__(kThreads, 3) enc_pack_kernel(const EncArgs<T> a)
 {
-    __shared__ alignas(16) uint8_t st[kStagingBytes];
-    __shared__ uint32_t off[kMaxTileBlocks];
-    __shared__ uint8_t hdr[kMaxTileBlocks];
-    __shared__ uint32_t wsum[kWarps];
-    __shared__ uint32_t br_rel[kMaxTileBlocks];
-    __shared__ uint8_t br_rows[kMaxTileBlocks];
+    extern __shared__ __align__(128) uint8_t pack_raw[];
+    PackSmem &sm = *reinterpret_cast<PackSmem *>(pack_raw);
     const Geom &g = a.g;
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, jb = lane & 7, r = lane >> 3;
     if (aborted(a.ctl)) return;  // pass 1 or the offsets failed: the stream is not written
     const unsigned long long t = blockIdx.x;
     const TileInfo ti = tile_info(g, t);
-    const unsigned long long ebase = tile_rows<T>(g, ti, br_rel, br_rows) * g.Z;
     {
         // block tid: header byte, size, offset inside the warp's 32 blocks
+        // (while the tile's input is fetched)
         const uint32_t h = tid < ti.nblk ? a.out[ti.k0 + tid] : 0u;
         const uint32_t sz = (h & 0x1fu) << (3u - (h >> 7));
         uint32_t inc = sz;
@@ -1959,14 +1966,17 @@ __global__ void __launch_bounds__(kThreads, 4) enc_pack_kernel(const EncArgs<T> 
             const uint32_t x = __shfl_up_sync(0xffffffffu, inc, o);
             if (lane >= (uint32_t)o) inc += x;
         }
-        hdr[tid] = (uint8_t)h;
-        off[tid] = inc - sz;
-        if (lane == 31) wsum[warp] = inc;
+        sm.hdr[tid] = (uint8_t)h;
+        sm.off[tid] = inc - sz;
+        if (lane == 31) sm.wsum[warp] = inc;
     }
-    __syncthreads();
+    if (!tile_in<T>(a, TileStage{sm.in, sm.mis, sm.br_rel, sm.br_rows}, &sm.full)) {
+        if (tid == 0) raise_error(a.ctl, DEV_ERR_TIMEOUT);
+        return;
+    }
     uint32_t wpre;  // lane w < kWarps: payload bytes of warps 0 .. w-1
     {
-        const uint32_t v = lane < (uint32_t)kWarps ? wsum[lane] : 0u;
+        const uint32_t v = lane < (uint32_t)kWarps ? sm.wsum[lane] : 0u;
         uint32_t inc = v;
 #pragma unroll
         for (int o = 1; o < kWarps; o <<= 1) {
@@ -1975,7 +1985,7 @@ __global__ void __launch_bounds__(kThreads, 4) enc_pack_kernel(const EncArgs<T> 
         }
         wpre = inc - v;
     }
-    const uint32_t agg = __shfl_sync(0xffffffffu, wpre, kWarps - 1) + wsum[kWarps - 1];
+    const uint32_t agg = __shfl_sync(0xffffffffu, wpre, kWarps - 1) + sm.wsum[kWarps - 1];
     const unsigned long long base = a.tile_off[t];
     if (g.R + base + agg > a.cap) {  // the same in every thread
         if (tid == 0) raise_error(a.ctl, DEV_ERR_CAPACITY);
@@ -1986,15 +1996,16 @@ __global__ void __launch_bounds__(kThreads, 4) enc_pack_kernel(const EncArgs<T> 
     for (uint32_t u = warp; u < nunits; u += kWarps) {
         const uint32_t b = u * 8 + jb;
         const bool active = b < ti.nblk;
+        const SegLoc L = seg_locate<T, true>(g, ti, sm.br_rel, sm.br_rows, sm.in, sm.mis, active ? b : 0u, r);
         Row<T> A, B;
-        tile_block_rows<T, VEC>(a.in, g, ti, br_rel, br_rows, ebase, b, active, r, A, B);
-        const uint32_t h = active ? hdr[b] : 0u;
-        const uint32_t o = off[active ? b : 0] + __shfl_sync(0xffffffffu, wpre, u >> 2);  // 4 units per 32 blocks
-        block_pack<T, BINS == BINS_IDENT>(A, B, h, active, r, xs, a.c, st + (active ? o : 0u));
+        load_rows<T, VEC>(L, active, r, A, B);
+        const uint32_t h = active ? sm.hdr[b] : 0u;
+        const uint32_t o = sm.off[active ? b : 0] + __shfl_sync(0xffffffffu, wpre, u >> 2);  // 4 units per 32 blocks
+        block_pack<T, BINS == BINS_IDENT>(A, B, h, active, r, xs, a.c, sm.st + (active ? o : 0u));
     }
     __syncthreads();
     {
-        const uint32_t *s32 = reinterpret_cast<const uint32_t *>(st);
+        const uint32_t *s32 = reinterpret_cast<const uint32_t *>(sm.st);
         uint32_t *d32 = reinterpret_cast<uint32_t *>(a.out + g.R + base);
         const uint32_t nw = agg / 4u;
         for (uint32_t w = tid; w < nw; w += kThreads) d32[w] = s32[w];
