@@ -262,9 +262,7 @@ int lscomp_plan_destroy(lscomp_plan *plan);
    previous mode.  lscomp_tune_report writes the table as text (one line per
    key: "es layout pool kind vec bzb -> shape tile_blocks", then
    " | shape tile_blocks ms" per timed candidate; kind 0 compress, 1 batch,
-   2 decompress; shape -1 = rule, 0 = 2x8, 1 = 2x7, 2 = 2x13, 3 = two-pass:
-   a statistics kernel, the offsets kernel and a packing kernel, single
-   stacks only) and returns the bytes
+   2 decompress; shape -1 = rule, 0 = 2x8, 1 = 2x7, 2 = 2x13) and returns the bytes
    needed including the terminating NUL.  lscomp_tune_save / _load write and
    read that text (load replaces the keys it names; a malformed file changes
    nothing and returns LSCOMP_ERR_ARG).  Single stacks of fewer than 4

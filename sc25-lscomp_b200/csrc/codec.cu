@@ -51,7 +51,6 @@ int compress_async_t(lscomp_workspace *ws, const T *d_in, uint32_t x, uint32_t y
         a.cap = cap;
         a.ctl = ws->ctl;
         a.state = ws->state;
-        a.tile_off = ws->state + ws->state_cap;  // the two-pass encoder's tile offsets
         a.epoch = ws->epoch;
         a.sizes_out = reinterpret_cast<unsigned long long *>(d_sizes);
         return launch_enc_any<T, false>(a, vec, layout, pool, cfg.shape, ws->sm_count, st);
@@ -370,10 +369,7 @@ extern "C" int lscomp_compress_u16_noalloc(const uint16_t *d_in, uint32_t x, uin
         TuneCfg t;
         Geom gt;
         const TuneKey key{2, (uint8_t)layout, (uint8_t)pool, kTuneCompress, (uint8_t)vec, a.g.bzb};
-        // (the two-pass encoder's offsets need more scratch than the fixed
-        // array is laid out for: that choice runs the persistent kernel here)
-        if (tune_lookup(key, t) && t.shape != kShapeTwoPass && make_geom(x, y, z, t.tile_blocks, gt) &&
-            gt.ntiles <= kNoAllocMaxTiles) {
+        if (tune_lookup(key, t) && make_geom(x, y, z, t.tile_blocks, gt) && gt.ntiles <= kNoAllocMaxTiles) {
             cfg = t;
             a.g = gt;
         }

@@ -566,8 +566,7 @@ int plan_create_t(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, 
     cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMalloc(&p->ctl, sizeof(LaunchCtl));
     if (e == cudaSuccess) e = cudaMallocHost(&p->h_ctl, sizeof(LaunchCtl));
-    // look-back words; then, for the two-pass encoder, ntiles + 1 tile offsets
-    if (e == cudaSuccess) e = cudaMalloc(&p->state, (2 * total + 1) * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc(&p->state, total * sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMalloc(&p->d_sizes, 2ull * n * sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMallocHost(&p->h_sizes, 2ull * n * sizeof(unsigned long long));
     if (e == cudaSuccess && n > 1) {
@@ -602,7 +601,6 @@ int plan_create_t(lscomp_workspace *ws, const lscomp_stack *stacks, uint32_t n, 
         a.c = c;
         a.ctl = p->ctl;
         a.state = p->state;
-        a.tile_off = p->state + total;
         a.epoch = kPlanEpoch;
         if (n == 1) {
             a.in = static_cast<const T *>(stacks[0].d_in);

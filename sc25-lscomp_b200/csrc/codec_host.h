@@ -237,50 +237,9 @@ inline double unit_fill(const Geom &g, uint32_t wpg)
 // / 2 x 13 (uint16; 2 x 13 for single stacks only; uint32 always runs 2 x 8).
 constexpr int kWideWpg = 13;
 
-// The two-pass encoder (single stacks): header bytes, per-tile offsets from
-// them (the decoder's offsets kernel, its look-back words in a.state), then
-// the packing; a.tile_off holds ntiles + 1 offsets.
-template <typename T, int VEC, int BINS, bool POOL>
-inline int launch_enc_2p(const EncArgs<T> &a, int sm_count, cudaStream_t st)
-{
-    if (a.g.ntiles > 0x7fffffffull || !a.tile_off) return LSCOMP_ERR_ARG;
-    enc_stats_kernel<T, VEC, BINS, POOL><<<(unsigned)a.g.ntiles, kThreads, 0, st>>>(a);
-    g_launches.fetch_add(1);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_status(e);
-    DecArgs<T> d = {};
-    d.g = a.g;
-    d.c = a.c;
-    d.in = a.out;  // the header bytes the statistics kernel wrote
-    d.cap = a.cap;
-    d.ctl = a.ctl;
-    d.state = a.state;
-    d.tile_off = a.tile_off;
-    d.epoch = a.epoch;
-    const unsigned long long nseg = (a.g.ntiles + kSegTiles - 1) / kSegTiles;
-    unsigned long long grid = (unsigned long long)sm_count * 4;
-    if (grid > nseg) grid = nseg;
-    dec_offsets_kernel<T><<<(unsigned)grid, kThreads, 0, st>>>(d);
-    g_launches.fetch_add(1);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_status(e);
-    auto pack = enc_pack_kernel<T, VEC, BINS, POOL>;
-    const size_t psmem = sizeof(PackSmem);
-    cudaFuncSetAttribute(pack, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem);
-    pack<<<(unsigned)a.g.ntiles, kThreads, psmem, st>>>(a);
-    g_launches.fetch_add(1);
-    return cuda_status(cudaGetLastError());
-}
-
-// shape 3: the two-pass encoder (single stacks; batch launches keep the
-// persistent kernel)
-constexpr int kShapeTwoPass = 3;
-
 template <typename T, int VEC, int BINS, bool POOL, bool BATCH>
 inline int launch_enc_t(const EncArgs<T> &a, int shape, int sm_count, cudaStream_t st)
 {
-    if constexpr (!BATCH)
-        if (shape == kShapeTwoPass) return launch_enc_2p<T, VEC, BINS, POOL>(a, sm_count, st);
     if constexpr (sizeof(T) == 2 && LSC_ENC_GROUPS == 2 && LSC_ENC_WPG == 8) {
         if (shape < 0 && BINS != BINS_IDENT && !BATCH) {
             const double f8 = unit_fill(a.g, 8), f7 = unit_fill(a.g, 7), f13 = unit_fill(a.g, kWideWpg);

@@ -123,7 +123,6 @@ struct EncArgs {
     unsigned long long cap;
     LaunchCtl *ctl;
     unsigned long long *state;
-    unsigned long long *tile_off;   // two-pass encoder: per-tile payload offsets (ntiles + 1)
     uint32_t epoch;
     unsigned long long *sizes_out;  // optional device copy of {stream_len, payload}
     // batch launches: the stacks, the stack of every tile (tiles of all
@@ -786,24 +785,21 @@ __device__ __forceinline__ unsigned long long tile_prefix(unsigned long long *st
 }
 
 // ---------------------------------------------------------------- encoder
-// Where one tile's input lands in shared memory: the staging bytes, the
-// byte misalignment of each copied range (mod 16), and the block-row table
-// (element offset of each block-row from the tile's first row, its rows).
-struct TileStage {
-    uint8_t *in;
-    uint32_t *mis;
-    uint32_t *br_rel;
-    uint8_t *br_rows;
-};
-
-// One warp, all lanes: the block-row table, range bookkeeping and TMA issue
-// of tile t into ts; the copies complete on `full`.  The block-row starts
-// of the tile are computed one per lane, so the warp's dependent chain is
-// that of a single block-row.
+// Producer warp, all lanes: the block-row table, range bookkeeping and TMA
+// issue of tile t into input slot s; the copies complete on `full`.  The
+// block-row starts of the tile are computed one per lane, so the warp's
+// dependent chain is that of a single block-row.
 template <typename T>
-__device__ void issue_tile(const Geom &g, const T *in, const TileStage &ts, unsigned long long t, uint64_t *full,
-                           uint32_t lane)
+__device__ void enc_issue(const Geom &g, const T *in, EncSmem &sm, int s, unsigned long long t, uint64_t *full,
+                          uint32_t lane)
 {
+    if (t == kMarker) {
+        if (lane == 0) {
+            sm.in_tile[s] = t;
+            mbar_arrive(full);
+        }
+        return;
+    }
     constexpr uint32_t ES = sizeof(T);
     const TileInfo ti = tile_info(g, t);
     // ranges: whole-row tiles -> 1 contiguous range; chunked -> one per row.
@@ -822,8 +818,8 @@ __device__ void issue_tile(const Geom &g, const T *in, const TileStage &ts, unsi
             }
             if (q0 == 0) r0 = __shfl_sync(0xffffffffu, rs, 0);
             if (q < ti.nbr) {
-                ts.br_rel[q] = (uint32_t)((rs - r0) * g.Z);
-                ts.br_rows[q] = (uint8_t)nrows;
+                sm.br_rel[s][q] = (uint32_t)((rs - r0) * g.Z);
+                sm.br_rows[s][q] = (uint8_t)nrows;
             }
             const uint32_t last = ti.nbr - q0;  // lane holding the end row in this pass
             if (last < 32u) rend = __shfl_sync(0xffffffffu, rs, last);
@@ -834,7 +830,7 @@ __device__ void issue_tile(const Geom &g, const T *in, const TileStage &ts, unsi
     } else {
         uint32_t rows;
         const unsigned long long r0 = brow_start(g, ti.rho0, rows);
-        if (lane == 0) ts.br_rows[0] = (uint8_t)rows;
+        if (lane == 0) sm.br_rows[s][0] = (uint8_t)rows;
         const uint32_t col0 = 8u * ti.c0;
         uint32_t col1 = 8u * (ti.c0 + ti.nblk);
         if (col1 > g.Z) col1 = g.Z;
@@ -849,11 +845,11 @@ __device__ void issue_tile(const Geom &g, const T *in, const TileStage &ts, unsi
     uintptr_t cs = 0, ce = 0;
     uint8_t *dst = nullptr;
     if (lane < nr) {
-        uint8_t *sb = ts.in + (g.chunked ? lane * kChunkPitch : 0u);
+        uint8_t *sb = sm.in[s] + (g.chunked ? lane * kChunkPitch : 0u);
         const uintptr_t ga = base + ES * es;
         const uintptr_t ge = ga + ES * ne;
         const uintptr_t gs = ga & ~(uintptr_t)15;
-        ts.mis[lane] = (uint32_t)(ga & 15);
+        sm.in_mis[s][lane] = (uint32_t)(ga & 15);
         cs = gs > A0 ? gs : A0;
         ce = (ge + 15) & ~(uintptr_t)15;
         if (ce > A1) ce = A1;
@@ -866,25 +862,13 @@ __device__ void issue_tile(const Geom &g, const T *in, const TileStage &ts, unsi
         for (uintptr_t p = (ga > A1 ? ga : A1); p < ge; p += ES)
             *reinterpret_cast<T *>(sb + (p - gs)) = *reinterpret_cast<const T *>(p);
     }
+    if (lane == 0) sm.in_tile[s] = t;
     fence_proxy_async_smem();
     tx = __reduce_add_sync(0xffffffffu, tx);
     __syncwarp();
     if (lane == 0) mbar_arrive_expect_tx(full, tx);
     __syncwarp();
     if (lane < nr && ce > cs) bulk_g2s(dst, reinterpret_cast<const void *>(cs), (uint32_t)(ce - cs), full);
-}
-
-// Producer warp, all lanes: tile t (or the end marker) into input slot s.
-template <typename T>
-__device__ void enc_issue(const Geom &g, const T *in, EncSmem &sm, int s, unsigned long long t, uint64_t *full,
-                          uint32_t lane)
-{
-    if (lane == 0) sm.in_tile[s] = t;
-    if (t == kMarker) {
-        if (lane == 0) mbar_arrive(full);
-        return;
-    }
-    issue_tile<T>(g, in, TileStage{sm.in[s], sm.in_mis[s], sm.br_rel[s], sm.br_rows[s]}, t, full, lane);
 }
 
 // Where a lane's two row segments (rows r and r+4 of tile-local block b)
@@ -1853,173 +1837,6 @@ __global__ void __launch_bounds__(kThreads, LSC_DEC_CTAS) dec_kernel(const DecAr
         uint32_t Y[NG][4];
         dec_load<T>(pay + (active ? o : 0u), h, r, Y);
         dec_unit<T, VEC, BATCH>(a, ti, sm, Y, h, b, r, ebase);
-    }
-}
-
-// ---------------------------------------------------------------- two-pass encoder
-// The same stream from three launches with no wait between CTAs: the
-// statistics kernel writes every block's header byte, dec_offsets_kernel
-// turns the header bytes into per-tile payload offsets (as for decoding),
-// and the pack kernel quantises and packs each tile into shared memory and
-// copies it to its offset.  The input is read twice, but each kernel is a
-// plain one-CTA-per-tile kernel: several CTAs per SM hide one another's
-// latencies, where the persistent single-pass encoder keeps one CTA per SM
-// busy with a long chain of per-tile hand-offs (ring barriers, look-back,
-// write-out).  Which of the two runs is the tuner's choice per shape.
-
-// Tile blockIdx.x's input into shared memory: warp 0 builds the block-row
-// table and issues the TMA bulk copies (issue_tile, as the persistent
-// encoder's producer does), every thread waits for them to land (bounded).
-// false if they did not land in time.
-template <typename T>
-__device__ __forceinline__ bool tile_in(const EncArgs<T> &a, const TileStage &ts, uint64_t *full)
-{
-    const uint32_t tid = threadIdx.x;
-    if (tid == 0) {
-        mbar_init(full, 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncthreads();
-    if (tid < 32) issue_tile<T>(a.g, a.in, ts, blockIdx.x, full, tid);
-    return __syncthreads_and(mbar_wait_landed(full, 0)) != 0;
-}
-
-// Pass 1: the header byte of every block of tile blockIdx.x
-// (lsCOMP/src/cuLSZ_kernel.cu:898-957), written to the stream.
-template <typename T, int VEC, int BINS, bool POOL>
-__global__ void __launch_bounds__(kThreads, 6) enc_stats_kernel(const EncArgs<T> a)
-{
-    __shared__ alignas(128) uint8_t in_s[kStageBytes];
-    __shared__ uint32_t mis_s[8];
-    __shared__ uint32_t br_rel[kMaxTileBlocks];
-    __shared__ uint8_t br_rows[kMaxTileBlocks];
-    __shared__ uint8_t hdr[kMaxTileBlocks];
-    __shared__ uint64_t full;
-    __shared__ uint32_t bad_s;
-    const Geom &g = a.g;
-    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, jb = lane & 7, r = lane >> 3;
-    if (tid == 0) bad_s = 0;
-    if (!tile_in<T>(a, TileStage{in_s, mis_s, br_rel, br_rows}, &full)) {
-        if (tid == 0) raise_error(a.ctl, DEV_ERR_TIMEOUT);
-        return;
-    }
-    const TileInfo ti = tile_info(g, blockIdx.x);
-    const uint32_t nunits = (ti.nblk + 7) >> 3;
-    uint32_t bad = 0;
-    for (uint32_t u = warp; u < nunits; u += kWarps) {
-        const uint32_t b = u * 8 + jb;
-        const bool active = b < ti.nblk;
-        const SegLoc L = seg_locate<T, true>(g, ti, br_rel, br_rows, in_s, mis_s, active ? b : 0u, r);
-        Row<T> A, B;
-        load_rows<T, VEC>(L, active, r, A, B);
-        uint32_t rb;
-        const uint32_t h =
-            block_header<T, BINS == BINS_IDENT ? BINS_EQUAL : BINS, POOL, BINS == BINS_IDENT>(A, B, a.c, rb);
-        if (active && r == 0) {
-            hdr[b] = (uint8_t)h;
-            bad |= rb;
-        }
-    }
-    if (__any_sync(0xffffffffu, bad != 0) && lane == 0) atomicOr(&bad_s, 1u);
-    __syncthreads();
-    if (tid < ti.nblk) a.out[ti.k0 + tid] = hdr[tid];
-    // a uint32 quotient >= 2^31 needs 32 planes, which the 5-bit rate field
-    // cannot hold
-    if (tid == 0 && bad_s) raise_error(a.ctl, DEV_ERR_RANGE);
-}
-
-// Shared memory of the packing kernel (dynamic: more than 48 KB).
-struct PackSmem {
-    alignas(128) uint8_t in[kStageBytes];
-    alignas(16) uint8_t st[kStagingBytes];
-    uint32_t mis[8];
-    uint32_t br_rel[kMaxTileBlocks];
-    uint8_t br_rows[kMaxTileBlocks];
-    uint32_t off[kMaxTileBlocks];
-    uint8_t hdr[kMaxTileBlocks];
-    uint32_t wsum[kWarps];
-    uint64_t full;
-};
-
-// Pass 2: tile blockIdx.x's bit planes (lsCOMP/src/cuLSZ_kernel.cu:1100-1276)
-// packed in shared memory at the in-tile offsets its header bytes give,
-// then copied to the stream at R + tile_off[t] with consecutive 4-byte
-// words per thread; the last tile writes the totals and the header pad.
-template <typename T, int VEC, int BINS, bool POOL>
-__global__ void __launch_bounds__(kThreads, 3) enc_pack_kernel(const EncArgs<T> a)
-{
-    extern __shared__ __align__(128) uint8_t pack_raw[];
-    PackSmem &sm = *reinterpret_cast<PackSmem *>(pack_raw);
-    const Geom &g = a.g;
-    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, jb = lane & 7, r = lane >> 3;
-    if (aborted(a.ctl)) return;  // pass 1 or the offsets failed: the stream is not written
-    const unsigned long long t = blockIdx.x;
-    const TileInfo ti = tile_info(g, t);
-    {
-        // block tid: header byte, size, offset inside the warp's 32 blocks
-        // (while the tile's input is fetched)
-        const uint32_t h = tid < ti.nblk ? a.out[ti.k0 + tid] : 0u;
-        const uint32_t sz = (h & 0x1fu) << (3u - (h >> 7));
-        uint32_t inc = sz;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t x = __shfl_up_sync(0xffffffffu, inc, o);
-            if (lane >= (uint32_t)o) inc += x;
-        }
-        sm.hdr[tid] = (uint8_t)h;
-        sm.off[tid] = inc - sz;
-        if (lane == 31) sm.wsum[warp] = inc;
-    }
-    if (!tile_in<T>(a, TileStage{sm.in, sm.mis, sm.br_rel, sm.br_rows}, &sm.full)) {
-        if (tid == 0) raise_error(a.ctl, DEV_ERR_TIMEOUT);
-        return;
-    }
-    uint32_t wpre;  // lane w < kWarps: payload bytes of warps 0 .. w-1
-    {
-        const uint32_t v = lane < (uint32_t)kWarps ? sm.wsum[lane] : 0u;
-        uint32_t inc = v;
-#pragma unroll
-        for (int o = 1; o < kWarps; o <<= 1) {
-            const uint32_t x = __shfl_up_sync(0xffffffffu, inc, o);
-            if (lane >= (uint32_t)o) inc += x;
-        }
-        wpre = inc - v;
-    }
-    const uint32_t agg = __shfl_sync(0xffffffffu, wpre, kWarps - 1) + sm.wsum[kWarps - 1];
-    const unsigned long long base = a.tile_off[t];
-    if (g.R + base + agg > a.cap) {  // the same in every thread
-        if (tid == 0) raise_error(a.ctl, DEV_ERR_CAPACITY);
-        return;
-    }
-    const XSel xs = xsel(r);
-    const uint32_t nunits = (ti.nblk + 7) >> 3;
-    for (uint32_t u = warp; u < nunits; u += kWarps) {
-        const uint32_t b = u * 8 + jb;
-        const bool active = b < ti.nblk;
-        const SegLoc L = seg_locate<T, true>(g, ti, sm.br_rel, sm.br_rows, sm.in, sm.mis, active ? b : 0u, r);
-        Row<T> A, B;
-        load_rows<T, VEC>(L, active, r, A, B);
-        const uint32_t h = active ? sm.hdr[b] : 0u;
-        const uint32_t o = sm.off[active ? b : 0] + __shfl_sync(0xffffffffu, wpre, u >> 2);  // 4 units per 32 blocks
-        block_pack<T, BINS == BINS_IDENT>(A, B, h, active, r, xs, a.c, sm.st + (active ? o : 0u));
-    }
-    __syncthreads();
-    {
-        const uint32_t *s32 = reinterpret_cast<const uint32_t *>(sm.st);
-        uint32_t *d32 = reinterpret_cast<uint32_t *>(a.out + g.R + base);
-        const uint32_t nw = agg / 4u;
-        for (uint32_t w = tid; w < nw; w += kThreads) d32[w] = s32[w];
-    }
-    if (t == g.ntiles - 1) {
-        if (tid == 0) {
-            a.ctl->total = base + agg;
-            a.ctl->stream_len = g.R + base + agg;
-            if (a.sizes_out) {
-                a.sizes_out[0] = g.R + base + agg;
-                a.sizes_out[1] = base + agg;
-            }
-        }
-        if (tid < (uint32_t)(g.R - g.nb)) a.out[g.nb + tid] = 0;  // header pad
     }
 }
 

@@ -53,13 +53,9 @@ bool valid_cfg(const TuneKey &k, const TuneCfg &c)
 {
     const uint32_t maxb = k.es == 2 ? 256u : 128u;
     if (c.tile_blocks < 8 || c.tile_blocks > maxb || c.tile_blocks % 8) return false;
-    if (c.shape < -1 || c.shape > kShapeTwoPass) return false;
-    if (c.shape == kShapeTwoPass) {
-        if (k.kind != kTuneCompress) return false;  // two-pass: single stacks, both element types
-    } else {
-        if (c.shape >= 1 && k.es != 2) return false;
-        if (c.shape == 2 && k.kind == kTuneBatch) return false;  // 2 x 13 runs single stacks only
-    }
+    if (c.shape < -1 || c.shape > 2) return false;
+    if (c.shape >= 1 && k.es != 2) return false;
+    if (c.shape == 2 && k.kind == kTuneBatch) return false;  // 2 x 13 runs single stacks only
     if (k.vec != 16 && k.vec != 4 && !(k.vec == 2 && k.es == 2)) return false;
     return k.es == 2 || k.es == 4;
 }
@@ -105,9 +101,8 @@ void tune_store(const TuneKey &k, const TuneCfg &c, const std::vector<std::pair<
 
 // Candidates per element size and call kind.  Encoder: CTA shape 2 x 8,
 // 2 x 7 or (single stacks) 2 x 13 warps (uint16) and tiles
-// of up to 256 or 128 blocks (uint16; 128 or 64 for uint32), and (single
-// stacks) the two-pass encoder with full tiles.  Decoder: tiles of 256 or
-// 128 (128 or 64) blocks.
+// of up to 256 or 128 blocks (uint16; 128 or 64 for uint32).  Decoder:
+// tiles of 256 or 128 (128 or 64) blocks.
 std::vector<TuneCfg> tune_candidates(int es, int kind)
 {
     const uint32_t big = es == 2 ? 256u : 128u, small = big / 2;
@@ -120,7 +115,6 @@ std::vector<TuneCfg> tune_candidates(int es, int kind)
     v.push_back({0, big});
     if (es == 2) v.push_back({1, big});
     if (es == 2 && kind == kTuneCompress) v.push_back({2, big});
-    if (kind == kTuneCompress) v.push_back({kShapeTwoPass, big});
     v.push_back({0, small});
     if (es == 2) v.push_back({1, small});
     return v;

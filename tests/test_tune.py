@@ -67,9 +67,7 @@ def test_table_roundtrip(lzc, tmp_path):
                     "4 1 1 0 2 9 -> 0 64\n", "2 1 1 0 8 9 -> 0 64\n",
                     "2 1 1 1 16 0 -> 2 256\n",   # 2 x 13 runs single stacks only
                     "4 1 1 0 16 9 -> 2 128\n",   # and uint16 only
-                    "2 1 1 1 16 0 -> 3 256\n",   # the two-pass encoder: single stacks only
-                    "2 3 0 2 16 128 -> 3 256\n",  # and compression only
-                    "2 1 1 0 16 9 -> 4 256\n"):
+                    "2 1 1 0 16 9 -> 3 256\n"):
             f.write_text("2 1 1 0 16 7 -> 0 8\n" + bad)
             with pytest.raises(lzc.LscompError):
                 lzc.tune_load(str(f))
@@ -124,9 +122,7 @@ def force(lz, tmp_path, line):
     lz.tune_load(str(f))
 
 
-# shape 0 / 1 / 2: the persistent encoder with 2 x 8 / 2 x 7 / 2 x 13 warps;
-# 3: the two-pass encoder (statistics, offsets, packing)
-CANDIDATES = {2: [(0, 256), (1, 256), (2, 256), (3, 256), (0, 128), (1, 128)], 4: [(0, 128), (3, 128), (0, 64)]}
+CANDIDATES = {2: [(0, 256), (1, 256), (2, 256), (0, 128), (1, 128)], 4: [(0, 128), (0, 64)]}
 DEC_CANDIDATES = {2: [(-1, 256), (-1, 128)], 4: [(-1, 128), (-1, 64)]}
 SHAPES = [(3, 37, 53), (2, 17, 2100), (4, 64, 1024), (2, 40, 1558), (1, 9, 2049)]
 
@@ -264,38 +260,6 @@ def test_plan_single_stack(lz, ws, oracle, es):
             d_in.copy_(to_dev(a))
     finally:
         plan.close()
-
-
-@pytest.mark.gpu
-@pytest.mark.parametrize("es", [2, 4])
-def test_plan_single_stack_two_pass(lz, ws, oracle, tmp_path, es):
-    """A plan of one stack whose key the table gives the two-pass encoder:
-    its three kernels are captured and replayed."""
-    dtype = np.uint16 if es == 2 else np.uint32
-    dims = (6, 181, 1558)
-    bins, p = LOSSY
-    prev = lz.tune_mode(1)
-    try:
-        force(lz, tmp_path, f"{es} {layout_of(bins)} {pool_of(p)} 0 {vec_of(dims[2], es)} {(dims[2] + 7) // 8} -> 3 "
-                            f"{256 if es == 2 else 128}")
-        a = random_stack(dims, seed=4, dtype=dtype)
-        d_in = to_dev(a)
-        out = torch.zeros(lz.max_stream_bytes(dims, es), dtype=torch.uint8, device="cuda")
-        plan = lz.Plan(ws, [(d_in, dims, out)], bins, p)
-        try:
-            for rnd in range(2):
-                out.fill_(0xEE)
-                (sl, rs), = plan.run()
-                s_o, rs_o = oracle.compress(a, dims, bins, p, dtype=dtype)
-                assert sl == len(s_o) and rs == rs_o
-                assert np.array_equal(out[:sl].cpu().numpy(), s_o)
-                a = random_stack(dims, seed=60 + rnd, dtype=dtype)
-                d_in.copy_(to_dev(a))
-        finally:
-            plan.close()
-    finally:
-        lz.tune_clear()
-        lz.tune_mode(prev)
 
 
 @pytest.mark.gpu
