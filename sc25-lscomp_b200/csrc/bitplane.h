@@ -79,6 +79,92 @@ LSC_HD void lsc_row_values(uint32_t l_lo, uint32_t l_hi, uint32_t h_lo, uint32_t
     w0 = lsc_prmt(l_hi, h_hi, 0x6273u);
 }
 
+// The first two rounds of lsc_transpose8x8 on one word: a 4x4 bit transpose
+// of the low nibbles (bit c of byte a <-> bit a of byte c, a, c < 4) and one
+// of the high nibbles.  Its own inverse.
+LSC_HD uint32_t lsc_transpose4x4x2(uint32_t x)
+{
+    uint32_t t;
+    t = (x ^ (x >> 7)) & 0x00AA00AAu; x ^= t ^ (t << 7);
+    t = (x ^ (x >> 14)) & 0x0000CCCCu; x ^= t ^ (t << 14);
+    return x;
+}
+
+// Values below 16: the 8 values of a row as nibbles of one word, byte a
+// holding q(7-a) in its low nibble and q(3-a) in its high nibble.
+LSC_HD uint32_t lsc_row_nibbles(uint32_t w0, uint32_t w1, uint32_t w2, uint32_t w3)
+{
+    return lsc_prmt(w3 | (w1 << 4), w2 | (w0 << 4), 0x4602u);
+}
+
+// Values below 16: planes 0-3 of a row (p_lo of lsc_row_planes, high=0).
+// With the high value nibbles zero, the third round of the 8x8 transpose
+// only merges the two halves, so it is done first, by lsc_row_nibbles.
+LSC_HD uint32_t lsc_row_planes4(uint32_t w0, uint32_t w1, uint32_t w2, uint32_t w3)
+{
+    return lsc_transpose4x4x2(lsc_row_nibbles(w0, w1, w2, w3));
+}
+
+// Values below 4, two rows a and b: bytes 0-3 = plane 0 of a, plane 1 of a,
+// plane 0 of b, plane 1 of b.  Row b's two bits sit above row a's in every
+// nibble, so one pair of 4x4 transposes serves both rows.
+LSC_HD uint32_t lsc_rows_planes2(const uint32_t a[4], const uint32_t b[4])
+{
+    const uint32_t na = lsc_row_nibbles(a[0], a[1], a[2], a[3]);
+    const uint32_t nb = lsc_row_nibbles(b[0], b[1], b[2], b[3]);
+    return lsc_transpose4x4x2(na | (nb << 2));
+}
+
+// Inverse of lsc_row_planes4: planes 0-3 of a row back to w0..w3.
+LSC_HD void lsc_row_values4(uint32_t p, uint32_t &w0, uint32_t &w1, uint32_t &w2, uint32_t &w3)
+{
+    const uint32_t x = lsc_transpose4x4x2(p);
+    const uint32_t L = x & 0x0f0f0f0fu, H = (x >> 4) & 0x0f0f0f0fu;  // q7 q6 q5 q4 / q3 q2 q1 q0
+    w3 = lsc_prmt(L, 0u, 0x4051u);
+    w2 = lsc_prmt(L, 0u, 0x6273u);
+    w1 = lsc_prmt(H, 0u, 0x4051u);
+    w0 = lsc_prmt(H, 0u, 0x6273u);
+}
+
+// Inverse of lsc_rows_planes2: rows a and b back from their planes 0 and 1.
+LSC_HD void lsc_rows_values2(uint32_t p, uint32_t a[4], uint32_t b[4])
+{
+    const uint32_t x = lsc_transpose4x4x2(p);
+    const uint32_t La = x & 0x03030303u, Ha = (x >> 4) & 0x03030303u;
+    const uint32_t Lb = (x >> 2) & 0x03030303u, Hb = (x >> 6) & 0x03030303u;
+    a[3] = lsc_prmt(La, 0u, 0x4051u);
+    a[2] = lsc_prmt(La, 0u, 0x6273u);
+    a[1] = lsc_prmt(Ha, 0u, 0x4051u);
+    a[0] = lsc_prmt(Ha, 0u, 0x6273u);
+    b[3] = lsc_prmt(Lb, 0u, 0x4051u);
+    b[2] = lsc_prmt(Lb, 0u, 0x6273u);
+    b[1] = lsc_prmt(Hb, 0u, 0x4051u);
+    b[0] = lsc_prmt(Hb, 0u, 0x6273u);
+}
+
+// Quotients of both 16-bit halves of w when every value is below 128:
+// floor(v / bin) = (v * m) >> s with m <= 511, so both products stay inside
+// their halves and one multiply serves the pair; the mask drops the bits the
+// high product shifts into the low half.  qsm = m | s << 16 from
+// lsc_small_quant_magic.
+LSC_HD uint32_t lsc_quant7x2(uint32_t w, uint32_t qsm)
+{
+    const uint32_t s = qsm >> 16;
+    return ((w * (qsm & 0xffffu)) >> s) & ((0xffffu >> s) | 0xffff0000u);
+}
+
+// m and s for lsc_quant7x2: s = bit length of 128 * bin - 1 (so 2^s >= 128 *
+// bin > 127 * (m * bin - 2^s), which makes the quotient exact for v < 128)
+// and m = ceil(2^s / bin); bins of 128 and more give 0 for every such value.
+LSC_HD uint32_t lsc_small_quant_magic(uint32_t bin)
+{
+    if (bin >= 128u) return 0u;
+    uint32_t s = 0;
+    while ((1u << s) < 128u * bin) s++;
+    const uint32_t m = ((1u << s) + bin - 1u) / bin;
+    return m | (s << 16);
+}
+
 // Byte selectors of the 4x4 byte transpose across four threads r = 0..3
 // (see xpose4 in the kernels).  Step A exchanges with thread r^2: threads 0,1
 // keep their bytes 0,1 and take the partner's bytes 0,1; threads 2,3 take the

@@ -264,7 +264,7 @@ __global__ void __launch_bounds__(kThreads) size_kernel(const BatchStack *stacks
             const uint32_t h =
                 block_header<T, BINS == BINS_IDENT ? BINS_EQUAL : BINS, POOL, BINS == BINS_IDENT>(A, B, bs.c, rb);
             if (active && r == 0) {
-                sum += (h & 0x1fu) << (3u - (h >> 7));  // rate planes of 8 bytes, or 4 when pooled
+                sum += (h & 0x1fu) << (3u - ((h >> 7) & 1u));  // rate planes of 8 bytes, or 4 when pooled
                 bad |= rb;
             }
         }

@@ -123,6 +123,7 @@ inline bool make_codec(const uint32_t bins[4], float p, bool wide, Codec &c, int
         c.magic[k] = bins[k] == 1 ? 0u : (uint32_t)((0x100000000ull + bins[k] - 1) / bins[k]);
         c.magic64[k] = magic64(bins[k]);
         c.binc[k] = (!wide && bins[k] > 65536u) ? 65536u : bins[k];
+        c.qsm[k] = lsc_small_quant_magic(bins[k]);
     }
     c.pool_min = pool_min_zeros(p);
     if (bins[0] == 1 && bins[1] == 1 && bins[2] == 1 && bins[3] == 1)

@@ -111,6 +111,7 @@ struct Codec {
     uint32_t magic[4];             // uint16: ceil(2^32 / bin) for bin >= 2, 0 for bin == 1
     unsigned long long magic64[4]; // uint32: ceil(2^64 / bin) for bin >= 2, 0 for bin == 1
     uint32_t binc[4];              // bins for the comparisons (uint16: clamped to 65536)
+    uint32_t qsm[4];               // uint16 values below 128: lsc_small_quant_magic(bin)
     int pool_min;                  // a block pools iff zero count >= pool_min (65: never)
 };
 
@@ -575,14 +576,22 @@ __device__ __forceinline__ uint32_t mul16x2(uint32_t w, uint32_t bin)
     return __byte_perm(w * bin, (w & 0xffff0000u) * bin, 0x7610u);
 }
 
-__device__ __forceinline__ void dequant(Row<uint16_t> &v, uint32_t bin)
+// both halves times bin when every product is known to stay below 2^16
+// (pair: the quantised values are below 2^rate and bin <= 2^16 >> rate): one
+// multiply, since the low product then carries nothing into the high half
+__device__ __forceinline__ uint32_t mul16x2_any(uint32_t w, uint32_t bin, bool pair)
+{
+    return pair ? w * bin : mul16x2(w, bin);
+}
+
+__device__ __forceinline__ void dequant(Row<uint16_t> &v, uint32_t bin, bool pair)
 {
     if (bin == 1u) return;
 #pragma unroll
-    for (int i = 0; i < 4; i++) v.w[i] = mul16x2(v.w[i], bin);
+    for (int i = 0; i < 4; i++) v.w[i] = mul16x2_any(v.w[i], bin, pair);
 }
 
-__device__ __forceinline__ void dequant(Row<uint32_t> &v, uint32_t bin)
+__device__ __forceinline__ void dequant(Row<uint32_t> &v, uint32_t bin, bool)
 {
 #pragma unroll
     for (int i = 0; i < 8; i++) v.w[i] *= bin;
@@ -590,10 +599,10 @@ __device__ __forceinline__ void dequant(Row<uint32_t> &v, uint32_t bin)
 
 // one output row from 4 pooled quantised values (the first half of q, or
 // the second): each value de-quantised and repeated over its two columns
-__device__ __forceinline__ Row<uint16_t> unpool_row(const Row<uint16_t> &q, bool second, uint32_t bin)
+__device__ __forceinline__ Row<uint16_t> unpool_row(const Row<uint16_t> &q, bool second, uint32_t bin, bool pair)
 {
     Row<uint16_t> v;
-    const uint32_t a = mul16x2(q.w[second ? 2 : 0], bin), b = mul16x2(q.w[second ? 3 : 1], bin);
+    const uint32_t a = mul16x2_any(q.w[second ? 2 : 0], bin, pair), b = mul16x2_any(q.w[second ? 3 : 1], bin, pair);
     v.w[0] = __byte_perm(a, 0u, 0x1010u);  // first value in both halves
     v.w[1] = __byte_perm(a, 0u, 0x3232u);  // second value in both halves
     v.w[2] = __byte_perm(b, 0u, 0x1010u);
@@ -601,7 +610,7 @@ __device__ __forceinline__ Row<uint16_t> unpool_row(const Row<uint16_t> &q, bool
     return v;
 }
 
-__device__ __forceinline__ Row<uint32_t> unpool_row(const Row<uint32_t> &q, bool second, uint32_t bin)
+__device__ __forceinline__ Row<uint32_t> unpool_row(const Row<uint32_t> &q, bool second, uint32_t bin, bool)
 {
     Row<uint32_t> v;
 #pragma unroll
@@ -1045,10 +1054,47 @@ __device__ __forceinline__ uint32_t block_header(const Row<T> &A, const Row<T> &
     return (pool ? 0x80u : 0u) | (choice << 5) | (rate & 0x1fu);
 }
 
+// A row quantised by the block's bin; small (warp-uniform): every value of
+// the unit is below 128, so one multiply quantises a pair of values.
+__device__ __forceinline__ void quant_row(Row<uint16_t> &v, const Codec &c, uint32_t choice, bool small)
+{
+    if (small) {
+        const uint32_t qsm = c.qsm[choice];
+#pragma unroll
+        for (int i = 0; i < 4; i++) v.w[i] = lsc_quant7x2(v.w[i], qsm);
+    } else {
+        quant(v, c, choice);
+    }
+}
+
+__device__ __forceinline__ void quant_row(Row<uint32_t> &v, const Codec &c, uint32_t choice, bool)
+{
+    quant(v, c, choice);
+}
+
+// One half (rows 0-3 in y1, rows 4-7 in y2) of plane pl of this lane's
+// block after the byte transpose, stored at dst.
+__device__ __forceinline__ void put_plane(uint8_t *dst, uint32_t y1, uint32_t y2, uint32_t pl, uint32_t rate,
+                                          bool pool, bool active)
+{
+    if (pool) {
+        y1 = __byte_perm(y1, 0, 0x3120);  // row pairs were taken in the order 0,2,1,3
+        if (active && pl < rate) *reinterpret_cast<uint32_t *>(dst + 4u * pl) = y1;
+    } else if (active && pl < rate) {
+        // block payloads start at multiples of 4 bytes only (a pooled block
+        // has 4 bytes per plane), so the plane pairs go out as two words
+        *reinterpret_cast<uint32_t *>(dst + 8u * pl) = y1;
+        *reinterpret_cast<uint32_t *>(dst + 8u * pl + 4u) = y2;
+    }
+}
+
 // Pass B for one unit: bit planes (lsCOMP/src/cuLSZ_kernel.cu:1100-1276) of
 // the block whose header is h, stored at dst (shared memory).  IDENT: every
-// bin is 1, values are their own quantisation.
-template <typename T, bool IDENT>
+// bin is 1, values are their own quantisation.  NARROW (uint16; callers
+// that inline this once, not once per unit): units of small values take
+// shorter paths -- pair quotients below 128, planes 0-3 only below 16, one
+// word for planes 0-1 of two rows below 4.
+template <typename T, bool IDENT, bool NARROW>
 __device__ __forceinline__ void block_pack(const Row<T> &A0, const Row<T> &B0, uint32_t h, bool active, uint32_t r,
                                            const XSel &xs, const Codec &c, uint8_t *dst)
 {
@@ -1062,12 +1108,14 @@ __device__ __forceinline__ void block_pack(const Row<T> &A0, const Row<T> &B0, u
     // blocks only (mostly-zero data) has no planes, so nothing is quantised
     const uint32_t wrate = __reduce_max_sync(0xffffffffu, rate);
     if (wrate == 0u) return;
+    const bool small = NARROW && !IDENT && sizeof(T) == 2 &&
+                       __all_sync(0xffffffffu, (or_all(A0) | or_all(B0)) < 128u);
     Row<T> A = A0, B = B0;
     if (__any_sync(0xffffffffu, active && pool)) {
         // pooled blocks: lane r=0 takes row pair (0,1), r=1 (4,5), r=2 (2,3),
         // r=3 (6,7) -- one pooled byte row each
         Row<T> P = pool_rows(A0, B0);
-        if (!IDENT) quant(P, c, choice);
+        if (!IDENT) quant_row(P, c, choice, small);
         Row<T> V;
 #pragma unroll
         for (int i = 0; i < NW / 2; i++) {
@@ -1081,12 +1129,36 @@ __device__ __forceinline__ void block_pack(const Row<T> &A0, const Row<T> &B0, u
 #pragma unroll
             for (int i = 0; i < NW; i++) B.w[i] = 0;
         } else if (!IDENT) {
-            quant(A, c, choice);
-            quant(B, c, choice);
+            quant_row(A, c, choice, small);
+            quant_row(B, c, choice, small);
         }
     } else if (!IDENT) {
-        quant(A, c, choice);
-        quant(B, c, choice);
+        quant_row(A, c, choice, small);
+        quant_row(B, c, choice, small);
+    }
+    if constexpr (NARROW && sizeof(T) == 2) {
+        if (wrate <= 2u) {
+            // every quantised value of the unit is below 4: planes 0 and 1 of
+            // rows r and r+4 in one word (bytes: row r plane 0, plane 1, row
+            // r+4 plane 0, plane 1), so one byte transpose leaves lane r with
+            // plane r&1 of rows 0-3 (r < 2) or rows 4-7 (r >= 2)
+            uint32_t y = xpose4(lsc_rows_planes2(A.w, B.w), xs);
+            const uint32_t pl = r & 1u;
+            if (pool) {
+                y = __byte_perm(y, 0, 0x3120);
+                if (active && r < 2u && pl < rate) *reinterpret_cast<uint32_t *>(dst + 4u * pl) = y;
+            } else if (active && pl < rate) {
+                *reinterpret_cast<uint32_t *>(dst + 8u * pl + 4u * (r >> 1)) = y;
+            }
+            return;
+        }
+        if (wrate <= 4u) {
+            // below 16: planes 0-3 only, from one word per row
+            const uint32_t y1 = xpose4(lsc_row_planes4(A.w[0], A.w[1], A.w[2], A.w[3]), xs);
+            const uint32_t y2 = xpose4(lsc_row_planes4(B.w[0], B.w[1], B.w[2], B.w[3]), xs);
+            put_plane(dst, y1, y2, r, rate, pool, active);
+            return;
+        }
     }
 #pragma unroll
     for (uint32_t grp = 0; grp < (uint32_t)NG; grp++) {
@@ -1095,25 +1167,9 @@ __device__ __forceinline__ void block_pack(const Row<T> &A0, const Row<T> &B0, u
         row_planes(A, grp, aL, aH);
         row_planes(B, grp, bL, bH);
         const uint32_t pl = 8u * grp + r;  // planes pl and pl + 4
-        uint32_t y1 = xpose4(aL, xs), y2 = xpose4(bL, xs);
-        if (pool) {
-            y1 = __byte_perm(y1, 0, 0x3120);  // row pairs were taken in the order 0,2,1,3
-            if (active && pl < rate) *reinterpret_cast<uint32_t *>(dst + 4u * pl) = y1;
-        } else if (active && pl < rate) {
-            // block payloads start at multiples of 4 bytes only (a pooled block
-            // has 4 bytes per plane), so the plane pairs go out as two words
-            *reinterpret_cast<uint32_t *>(dst + 8u * pl) = y1;
-            *reinterpret_cast<uint32_t *>(dst + 8u * pl + 4u) = y2;
-        }
+        put_plane(dst, xpose4(aL, xs), xpose4(bL, xs), pl, rate, pool, active);
         if (wrate <= 8u * grp + 4u) break;  // planes 8 grp + 4.. are empty in the whole unit
-        uint32_t y3 = xpose4(aH, xs), y4 = xpose4(bH, xs);
-        if (pool) {
-            y3 = __byte_perm(y3, 0, 0x3120);
-            if (active && pl + 4u < rate) *reinterpret_cast<uint32_t *>(dst + 4u * (pl + 4u)) = y3;
-        } else if (active && pl + 4u < rate) {
-            *reinterpret_cast<uint32_t *>(dst + 8u * (pl + 4u)) = y3;
-            *reinterpret_cast<uint32_t *>(dst + 8u * (pl + 4u) + 4u) = y4;
-        }
+        put_plane(dst, xpose4(aH, xs), xpose4(bH, xs), pl + 4u, rate, pool, active);
     }
 }
 
@@ -1171,31 +1227,47 @@ __device__ __forceinline__ void enc_compute(const EncArgs<T> &a, EncSmem &sm)
         const TileInfo ti = tile_info(g, t);
         const uint8_t *stage = sm.in[i];
 
-        // ---- pass A: rows to registers, header bytes
+        // ---- pass A: rows to registers (RELOAD: not kept), header bytes
         const uint32_t nunits = (ti.nblk + 7) >> 3;
         Row<T> A[UKEEP], B[UKEEP];
-        uint32_t hq[UMAX];
+        uint32_t hq[UKEEP];
         uint32_t bad = 0;
-#pragma unroll
-        for (int q = 0; q < UMAX; q++) {
-            const uint32_t u = wg + (uint32_t)q * WPG;
-            hq[q] = 0;
-            if (u < nunits) {
-                const uint32_t b = u * 8 + jb;
-                const bool active = b < ti.nblk;
-                SegLoc L = seg_locate<T, true>(g, ti, sm.br_rel[i], sm.br_rows[i], stage, sm.in_mis[i], active ? b : 0, r);
+        // rows r and r+4 of this lane's block of unit u, from the input slot
+        auto load_unit = [&](uint32_t u, Row<T> &ra, Row<T> &rb_) {
+            const uint32_t b = u * 8 + jb;
+            const bool active = b < ti.nblk;
+            SegLoc L = seg_locate<T, true>(g, ti, sm.br_rel[i], sm.br_rows[i], stage, sm.in_mis[i], active ? b : 0, r);
+            if constexpr (BATCH) load_rows_any<T>(L, active, r, ra, rb_, g.vec);
+            else load_rows<T, VEC>(L, active, r, ra, rb_);
+        };
+        auto header_unit = [&](uint32_t u, const Row<T> &ra, const Row<T> &rb_) -> uint32_t {
+            const uint32_t b = u * 8 + jb;
+            uint32_t rb;
+            const uint32_t h =
+                block_header<T, BINS == BINS_IDENT ? BINS_EQUAL : BINS, POOL, BINS == BINS_IDENT>(ra, rb_, cA, rb);
+            if (b < ti.nblk && r == 0) {
+                hdr[b] = (uint8_t)h;
+                bad |= rb;
+            }
+            return h;
+        };
+        if constexpr (RELOAD) {
+            // one copy of the unit code (the instruction cache holds the
+            // whole loop); the rows are read again in pass B
+#pragma unroll 1
+            for (uint32_t u = wg; u < nunits; u += WPG) {
                 Row<T> ra, rb_;
-                if constexpr (BATCH) load_rows_any<T>(L, active, r, ra, rb_, g.vec);
-                else load_rows<T, VEC>(L, active, r, ra, rb_);
-                if (!RELOAD) {
-                    A[RELOAD ? 0 : q] = ra;
-                    B[RELOAD ? 0 : q] = rb_;
-                }
-                uint32_t rb;
-                hq[q] = block_header<T, BINS == BINS_IDENT ? BINS_EQUAL : BINS, POOL, BINS == BINS_IDENT>(ra, rb_, cA, rb);
-                if (active && r == 0) {
-                    hdr[b] = (uint8_t)hq[q];
-                    bad |= rb;
+                load_unit(u, ra, rb_);
+                header_unit(u, ra, rb_);
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < UKEEP; q++) {
+                const uint32_t u = wg + (uint32_t)q * WPG;
+                hq[q] = 0;
+                if (u < nunits) {
+                    load_unit(u, A[q], B[q]);
+                    hq[q] = header_unit(u, A[q], B[q]);
                 }
             }
         }
@@ -1221,25 +1293,28 @@ __device__ __forceinline__ void enc_compute(const EncArgs<T> &a, EncSmem &sm)
         if (gtid == 0) free_ok = st_slot_free(sm, k, a.ctl);
         if (!group_bar_and(barid, WPG * 32, free_ok)) break;
 
-        // ---- pass B: pack from registers into the payload ring
+        // ---- pass B: pack (from registers, or RELOAD: from the input slot) into the payload ring
         uint8_t *const st = sm.st[j];
-#pragma unroll
-        for (int q = 0; q < UMAX; q++) {
-            const uint32_t u = wg + (uint32_t)q * WPG;
-            if (u < nunits) {
+        if constexpr (RELOAD) {
+#pragma unroll 1
+            for (uint32_t u = wg; u < nunits; u += WPG) {
                 const uint32_t b = u * 8 + jb;
                 const bool active = b < ti.nblk;
                 Row<T> ra, rb_;
-                if (RELOAD) {
-                    SegLoc L = seg_locate<T, true>(g, ti, sm.br_rel[i], sm.br_rows[i], stage, sm.in_mis[i],
-                                                   active ? b : 0, r);
-                    if constexpr (BATCH) load_rows_any<T>(L, active, r, ra, rb_, g.vec);
-                    else load_rows<T, VEC>(L, active, r, ra, rb_);
-                } else {
-                    ra = A[RELOAD ? 0 : q];
-                    rb_ = B[RELOAD ? 0 : q];
+                load_unit(u, ra, rb_);
+                block_pack<T, BINS == BINS_IDENT, true>(ra, rb_, active ? (uint32_t)hdr[b] : 0u, active, r, xs, cB,
+                                                        st + (active ? off[b] : 0u));
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < UKEEP; q++) {
+                const uint32_t u = wg + (uint32_t)q * WPG;
+                if (u < nunits) {
+                    const uint32_t b = u * 8 + jb;
+                    const bool active = b < ti.nblk;
+                    block_pack<T, BINS == BINS_IDENT, false>(A[q], B[q], hq[q], active, r, xs, cB,
+                                                             st + (active ? off[b] : 0u));
                 }
-                block_pack<T, BINS == BINS_IDENT>(ra, rb_, hq[q], active, r, xs, cB, st + (active ? off[b] : 0u));
             }
         }
         if (RELOAD) {
@@ -1584,12 +1659,26 @@ __global__ void __launch_bounds__(kThreads) dec_offsets_batch_kernel(const DecAr
 
 // Plane words of one block for this lane (planes 8 grp + r and 8 grp + r + 4;
 // words 1 and 3 hold rows 4-7 of a plain block).  Loads only planes < rate.
+// uint16: Z is the word a unit whose largest rate is at most 2 decodes from
+// -- plane r&1 of rows 0-3 (r < 2) or rows 4-7 (r >= 2), what the encoder's
+// single byte transpose of such a unit wrote.  It is loaded whatever the
+// unit's rates: no load waits for the unit's largest rate, and a branch on
+// it here cost more than the extra load.
 template <typename T>
-__device__ __forceinline__ void dec_load(const uint8_t *src, uint32_t h, uint32_t r, uint32_t Y[][4])
+__device__ __forceinline__ void dec_load(const uint8_t *src, uint32_t h, uint32_t r, uint32_t Y[][4], uint32_t &Z)
 {
     constexpr int NG = Elem<T>::kGroups;
     const bool pool = (h & 0x80u) != 0;
     const uint32_t rate = h & 0x1fu;
+    Z = 0;
+    if (sizeof(T) == 2) {
+        const uint32_t pl = r & 1u;
+        if (pool) {
+            if (r < 2u && pl < rate) Z = *reinterpret_cast<const uint32_t *>(src + 4u * pl);
+        } else if (pl < rate) {
+            Z = *reinterpret_cast<const uint32_t *>(src + 8u * pl + 4u * (r >> 1));
+        }
+    }
 #pragma unroll
     for (int grp = 0; grp < NG; grp++) {
         Y[grp][0] = Y[grp][1] = Y[grp][2] = Y[grp][3] = 0;
@@ -1612,42 +1701,61 @@ __device__ __forceinline__ void dec_load(const uint8_t *src, uint32_t h, uint32_
 
 // Values of rows r (A) and r+4 (B) of this lane's block from the unit's
 // plane words: transposes back, pooled rows expanded, de-quantised by the
-// header's bin.  All 32 lanes of the warp take part (one unit).
+// header's bin.  All 32 lanes of the warp take part (one unit); wrate is
+// the unit's largest rate.
 template <typename T>
-__device__ __forceinline__ void dec_values(uint32_t Y[][4], uint32_t h, bool active, uint32_t r, uint32_t bin,
-                                           Row<T> &A, Row<T> &B)
+__device__ __forceinline__ void dec_values(uint32_t Y[][4], uint32_t Z, uint32_t h, bool active, uint32_t r,
+                                           uint32_t bin, uint32_t wrate, Row<T> &A, Row<T> &B)
 {
     constexpr int NW = Elem<T>::kWords;
     constexpr int NG = Elem<T>::kGroups;
     const bool even = (r & 1u) == 0;
     const bool pool = (h & 0x80u) != 0;
-    const uint32_t wrate = __reduce_max_sync(0xffffffffu, h & 0x1fu);
     if (wrate == 0u) {  // every block of the unit has rate 0: all values are 0
 #pragma unroll
         for (int i = 0; i < NW; i++) A.w[i] = B.w[i] = 0;
         return;
     }
     const XSel xs = xsel(r);
-    // plane bytes per byte group, back in row order: [grp][0/1] = lo/hi half
-    // of row r (PA) and of row r+4 (PB); groups and halves above the unit's
-    // largest rate stay zero without any shuffles
-    uint32_t PA[NG][2], PB[NG][2];
-#pragma unroll
-    for (int grp = 0; grp < NG; grp++) {
-        PA[grp][0] = PA[grp][1] = PB[grp][0] = PB[grp][1] = 0;
-        if (wrate <= 8u * grp) continue;
-        uint32_t y1 = Y[grp][0];
-        if (pool) y1 = __byte_perm(y1, 0, 0x3120);  // undo the row-pair order 0,2,1,3
-        PA[grp][0] = xpose4(y1, xs);
-        PB[grp][0] = xpose4(Y[grp][1], xs);
-        if (wrate <= 8u * grp + 4u) continue;
-        uint32_t y3 = Y[grp][2];
-        if (pool) y3 = __byte_perm(y3, 0, 0x3120);
-        PA[grp][1] = xpose4(y3, xs);
-        PB[grp][1] = xpose4(Y[grp][3], xs);
+    bool narrow = false;
+    if constexpr (sizeof(T) == 2) {
+        if (wrate <= 2u) {
+            // one word: rows r and r+4, planes 0 and 1 (dec_load's Z)
+            if (pool) Z = __byte_perm(Z, 0, 0x3120);  // undo the row-pair order 0,2,1,3
+            lsc_rows_values2(xpose4(Z, xs), A.w, B.w);
+            narrow = true;
+        } else if (wrate <= 4u) {
+            uint32_t y1 = Y[0][0];
+            if (pool) y1 = __byte_perm(y1, 0, 0x3120);  // undo the row-pair order 0,2,1,3
+            lsc_row_values4(xpose4(y1, xs), A.w[0], A.w[1], A.w[2], A.w[3]);
+            lsc_row_values4(xpose4(Y[0][1], xs), B.w[0], B.w[1], B.w[2], B.w[3]);
+            narrow = true;
+        }
     }
-    row_values(PA, A, wrate);
-    row_values(PB, B, wrate);
+    if (!narrow) {
+        // plane bytes per byte group, back in row order: [grp][0/1] = lo/hi
+        // half of row r (PA) and of row r+4 (PB); groups and halves above the
+        // unit's largest rate stay zero without any shuffles
+        uint32_t PA[NG][2], PB[NG][2];
+#pragma unroll
+        for (int grp = 0; grp < NG; grp++) {
+            PA[grp][0] = PA[grp][1] = PB[grp][0] = PB[grp][1] = 0;
+            if (wrate <= 8u * grp) continue;
+            uint32_t y1 = Y[grp][0];
+            if (pool) y1 = __byte_perm(y1, 0, 0x3120);  // undo the row-pair order 0,2,1,3
+            PA[grp][0] = xpose4(y1, xs);
+            PB[grp][0] = xpose4(Y[grp][1], xs);
+            if (wrate <= 8u * grp + 4u) continue;
+            uint32_t y3 = Y[grp][2];
+            if (pool) y3 = __byte_perm(y3, 0, 0x3120);
+            PA[grp][1] = xpose4(y3, xs);
+            PB[grp][1] = xpose4(Y[grp][3], xs);
+        }
+        row_values(PA, A, wrate);
+        row_values(PB, B, wrate);
+    }
+    // products below 2^16 in every block of the unit: one multiply per pair
+    const bool pair = sizeof(T) == 2 && __all_sync(0xffffffffu, bin <= (0x10000u >> (h & 0x1fu)));
     if (__any_sync(0xffffffffu, active && pool)) {
         // a pooled lane holds the 8 pooled values of its row pair: 4 of the
         // first row, then 4 of the second.  Even lanes keep the first row and
@@ -1660,13 +1768,13 @@ __device__ __forceinline__ void dec_values(uint32_t Y[][4], uint32_t h, bool act
             Q.w[NW / 2 + i] = even ? t0 : A.w[NW / 2 + i];  // row r+4
         }
         if (pool) {
-            A = unpool_row(Q, false, bin);
-            B = unpool_row(Q, true, bin);
+            A = unpool_row(Q, false, bin, pair);
+            B = unpool_row(Q, true, bin, pair);
         }
     }
     if (!pool) {
-        dequant(A, bin);
-        dequant(B, bin);
+        dequant(A, bin, pair);
+        dequant(B, bin, pair);
     }
 }
 
@@ -1683,13 +1791,14 @@ __device__ __forceinline__ void store8_any(T *p, const Row<T> &v, uint32_t ncols
 // and r+4 of block b (BATCH: with the stack's own row access width).
 template <typename T, int VEC, bool BATCH>
 __device__ __forceinline__ void dec_unit(const DecArgs<T> &a, const TileInfo &ti, const DecSmem &sm, uint32_t Y[][4],
-                                         uint32_t h, uint32_t b, uint32_t r, unsigned long long ebase)
+                                         uint32_t Z, uint32_t h, uint32_t wrate, uint32_t b, uint32_t r,
+                                         unsigned long long ebase)
 {
     const Geom &g = a.g;
     const bool active = b < ti.nblk;
     SegLoc L = seg_locate<T, false>(g, ti, sm.br_rel, sm.br_rows, nullptr, nullptr, active ? b : 0, r);
     Row<T> A, B;
-    dec_values<T>(Y, h, active, r, a.c.bins[(h >> 5) & 3u], A, B);
+    dec_values<T>(Y, Z, h, active, r, a.c.bins[(h >> 5) & 3u], wrate, A, B);
     if (active) {
         T *rowA = a.out + ebase + L.growA;
         if constexpr (BATCH) {
@@ -1834,9 +1943,10 @@ __global__ void __launch_bounds__(kThreads, LSC_DEC_CTAS) dec_kernel(const DecAr
         const bool active = b < ti.nblk;
         const uint32_t h = active ? sm.hdr[b] : 0u;
         const uint32_t o = sm.off[active ? b : 0] + __shfl_sync(0xffffffffu, wpre, u >> 2);  // 4 units per warp's 32 blocks
-        uint32_t Y[NG][4];
-        dec_load<T>(pay + (active ? o : 0u), h, r, Y);
-        dec_unit<T, VEC, BATCH>(a, ti, sm, Y, h, b, r, ebase);
+        uint32_t Y[NG][4], Z;
+        dec_load<T>(pay + (active ? o : 0u), h, r, Y, Z);
+        const uint32_t wrate = __reduce_max_sync(0xffffffffu, h & 0x1fu);  // the unit's largest rate
+        dec_unit<T, VEC, BATCH>(a, ti, sm, Y, Z, h, wrate, b, r, ebase);
     }
 }
 

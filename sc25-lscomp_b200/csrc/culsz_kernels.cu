@@ -63,6 +63,7 @@ __device__ bool device_codec(const uint4 qb, float p, bool wide, Codec &c)
         c.magic[k] = v == 1u ? 0u : (uint32_t)((0x100000000ull + v - 1) / v);
         c.magic64[k] = v < 2u ? 0ull : ~0ull / v + 1;
         c.binc[k] = (!wide && v > 65536u) ? 65536u : v;
+        c.qsm[k] = lsc_small_quant_magic(v);
     }
     c.pool_min = 65;
     for (int k = 0; k <= 64; k++)
@@ -242,7 +243,7 @@ __device__ void compress_runs(const T *in, unsigned char *out, volatile OffT *cm
             unsigned long long e0;
             uint32_t nrows, ncols;
             block_rows<T>(in, d, byb, bzb, active ? b : 0u, active, r, A, B, e0, nrows, ncols);
-            block_pack<T, false>(A, B, hdr[i], active, r, xs, c, out + base + (active ? off[i] : 0u));
+            block_pack<T, false, false>(A, B, hdr[i], active, r, xs, c, out + base + (active ? off[i] : 0u));
         }
         if ((uint32_t)t == grid - 1) {
             if (lane == 0) cmpOffset[grid] = (OffT)(base - R + agg);  // the payload of the whole stream
@@ -282,10 +283,11 @@ __device__ void decompress_runs(T *outv, const unsigned char *in, volatile OffT 
             const uint32_t i = u * 8u + jb, b = k0 + i;
             const bool active = b < nb;
             const uint32_t h = hdr[i];
-            uint32_t Y[NG][4];
-            dec_load<T>(in + base + (active ? off[i] : 0u), h, r, Y);
+            uint32_t Y[NG][4], Z;
+            dec_load<T>(in + base + (active ? off[i] : 0u), h, r, Y, Z);
+            const uint32_t wrate = __reduce_max_sync(0xffffffffu, h & 0x1fu);
             Row<T> A, B;
-            dec_values<T>(Y, h, active, r, c.bins[(h >> 5) & 3u], A, B);
+            dec_values<T>(Y, Z, h, active, r, c.bins[(h >> 5) & 3u], wrate, A, B);
             if (!active) continue;
             const uint32_t per = byb * bzb;
             const uint32_t x = b / per, rem = b - x * per, by = rem / bzb, bz = rem - by * bzb;

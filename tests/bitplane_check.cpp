@@ -38,6 +38,47 @@ int main(void)
         lsc_row_values(a, b, c, d, r0, r1, r2, r3);
         bad += (r0 != w0) + (r1 != w1) + (r2 != w2) + (r3 != w3);
     }
+    // narrow values: planes 0-3 of values below 16, planes 0-1 of two rows
+    // of values below 4, and back
+    for (int it = 0; it < 200000; it++) {
+        uint32_t q[8], u[8];
+        for (int k = 0; k < 8; k++) {
+            q[k] = rnd() & 0xfu;
+            u[k] = rnd() & 0x3u;
+        }
+        const uint32_t w[4] = {q[0] | q[1] << 16, q[2] | q[3] << 16, q[4] | q[5] << 16, q[6] | q[7] << 16};
+        const uint32_t v[4] = {u[0] | u[1] << 16, u[2] | u[3] << 16, u[4] | u[5] << 16, u[6] | u[7] << 16};
+        uint32_t plo, phi;
+        lsc_row_planes(w[0], w[1], w[2], w[3], 0, plo, phi);
+        bad += lsc_row_planes4(w[0], w[1], w[2], w[3]) != plo;
+        uint32_t r0, r1, r2, r3;
+        lsc_row_values4(plo, r0, r1, r2, r3);
+        bad += (r0 != w[0]) + (r1 != w[1]) + (r2 != w[2]) + (r3 != w[3]);
+        // two rows: w's two low bits as row a, v as row b
+        uint32_t a2[4], ra[4], rb[4];
+        for (int i = 0; i < 4; i++) a2[i] = w[i] & 0x00030003u;
+        const uint32_t m = lsc_rows_planes2(a2, v);
+        for (int i = 0; i < 4; i++) {
+            const uint32_t *src = i < 2 ? a2 : v;
+            const int plane = i & 1;
+            uint32_t want = 0;
+            for (int k = 0; k < 8; k++)
+                want |= ((((src[k >> 1] >> (16 * (k & 1))) & 0xffffu) >> plane) & 1u) << (7 - k);
+            bad += ((m >> (8 * i)) & 0xffu) != want;
+        }
+        lsc_rows_values2(m, ra, rb);
+        for (int i = 0; i < 4; i++) bad += (ra[i] != a2[i]) + (rb[i] != v[i]);
+    }
+    // the paired quotient of values below 128, every bin it serves
+    for (uint32_t bin = 1; bin < 300; bin++) {
+        const uint32_t qsm = lsc_small_quant_magic(bin);
+        bad += (qsm & 0xffffu) > 511u;
+        for (uint32_t x = 0; x < 128; x++)
+            for (uint32_t y = 0; y < 128; y += 7) {
+                const uint32_t got = lsc_quant7x2(x | y << 16, qsm);
+                bad += got != ((x / bin) | (y / bin) << 16);
+            }
+    }
     for (int it = 0; it < 10000; it++) {
         uint32_t x[4], z[4], y[4];
         for (int r = 0; r < 4; r++) x[r] = rnd();
