@@ -765,8 +765,8 @@ def main():
     roofline = {"bound": "hbm", "kernel": k_dom, "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                 "frac": round(achieved / hbm, 4), "peak_kind": peak_kind,
                 "traffic": None, "algorithmic_bytes_per_launch": b_dom}
-    prof = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(prof):
+    prof = os.path.join(ROOT, "profiles", "traffic.json")  # measured on the default stack only
+    if os.path.exists(prof) and args.dims is None and args.kind == "cssi":
         try:
             tr = json.load(open(prof)).get(k_dom)
             if tr:
@@ -851,10 +851,27 @@ def bench_e2e(args, dims, ws, h, dev, nbytes, sizes, world, expect):
     e1.record(stream)
     torch.cuda.synchronize()
     ms = max_over_ranks(e0.elapsed_time(e1), world) / args.e2e_steps
+    # the link this box gives: one plain copy of the pinned stack each way;
+    # the floor a pass can reach is its larger direction at these rates
+    d_tmp = torch.empty_like(h_in, device=dev)
+    rates = {}
+    for way, (dst, src) in (("h2d", (d_tmp, h_in)), ("d2h", (h_out, d_tmp))):
+        dst.copy_(src, non_blocking=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        dst.copy_(src, non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        rates[way] = nbytes / (e0.elapsed_time(e1) / 1e3) / 1e9
+    del d_tmp
+    floor = sum(max(nbytes / rates["h2d"], sizes[m[0]] / rates["d2h"]) +
+                max(sizes[m[0]] / rates["h2d"], nbytes / rates["d2h"]) for m in MODES) / 1e6
     return {"value": round(world * 4 * nbytes / (ms / 1e3) / 1e9, 2), "unit": "GB/s",
             "h2d_bytes_per_step": int(moved["h2d"]), "d2h_bytes_per_step": int(moved["d2h"]),
             "ms_per_step": round(ms, 3), "checked": "streams and decodes equal the device-memory calls' (both modes)",
-            "path": "lscomp_compress_host_u16 / lscomp_decompress_host_u16 (C ABI), pinned host buffers"}
+            "path": "lscomp_compress_host_u16 / lscomp_decompress_host_u16 (C ABI), pinned host buffers",
+            "pcie_copy_gbs": {k: round(v, 1) for k, v in rates.items()},
+            "pcie_floor_ms_per_step": round(floor, 3)}
 
 
 def codec_ours(ws, lscomp, dims):
@@ -1080,25 +1097,39 @@ def bench_reference_gpu(args, dims, dev, d_in, d_cmp, d_dec, nbytes, config, h):
             sizes[name] = ref.compress(d_in.data_ptr(), d_cmp.data_ptr(), dims, bins, p)
             torch.cuda.synchronize()
 
-        def step():
-            for name, bins, p in MODES:
+        def step(ev=None):
+            for i, (name, bins, p) in enumerate(MODES):
+                if ev is not None:
+                    ev[3 * i].record(stream)
                 ref.compress(d_in.data_ptr(), d_cmp.data_ptr(), dims, bins, p)
+                if ev is not None:
+                    ev[3 * i + 1].record(stream)
                 ref.decompress(d_dec.data_ptr(), d_cmp.data_ptr(), sizes[name], dims, bins, p)
+                if ev is not None:
+                    ev[3 * i + 2].record(stream)
 
         for _ in range(max(args.warmup, 3)):
             step()
         torch.cuda.synchronize()
+        evs = [[torch.cuda.Event(enable_timing=True) for _ in range(6)] for _ in range(steps)]
         if clocks:
             clocks.start()
         e0.record(stream)
-        for _ in range(steps):
-            step()
+        for k in range(steps):
+            step(evs[k])
         e1.record(stream)
         torch.cuda.synchronize()
         clk = clocks.stop() if clocks else None
-        return e0.elapsed_time(e1) / steps, sizes, clk
+        # per pass, each call's own interval (the reference's calls
+        # allocate, clear, free and read back inside it)
+        per = {}
+        for i, (name, _, _) in enumerate(MODES):
+            per[name] = {"compress_ms": round(float(np.mean([e[3 * i].elapsed_time(e[3 * i + 1]) for e in evs])), 4),
+                         "decompress_ms": round(float(np.mean([e[3 * i + 1].elapsed_time(e[3 * i + 2])
+                                                               for e in evs])), 4)}
+        return e0.elapsed_time(e1) / steps, sizes, clk, per
 
-    ms, sizes, clk = run(ref, args.steps, ClockSampler(torch.cuda.current_device()))
+    ms, sizes, clk, per_mode = run(ref, args.steps, ClockSampler(torch.cuda.current_device()))
     value = 4 * nbytes / (ms / 1e3) / 1e9
     e2e = None
     if args.e2e_steps > 0:
@@ -1150,7 +1181,7 @@ def bench_reference_gpu(args, dims, dev, d_in, d_cmp, d_dec, nbytes, config, h):
                                        "the reference has no CPU "
                                        "implementation (bench.py --impl reference --ref-cpu times the C/OpenMP "
                                        "oracle on the host cores)"},
-            "e2e": e2e, "per_config": per_config}
+            "e2e": e2e, "per_mode": per_mode, "per_config": per_config}
 
 
 if __name__ == "__main__":
