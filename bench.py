@@ -532,7 +532,7 @@ def bench_batch(args, local):
 def tuned_summary(lscomp, kinds=("compress", "batch", "decompress")):
     """The tuner's choices so far: key -> chosen shape/tile size and the
     candidates' measured ms per call."""
-    shapes = {-1: "rule", 0: "2x8", 1: "2x7", 2: "2x13"}
+    shapes = {-1: "rule", 0: "2x8", 1: "2x7", 2: "2x13", 3: "2x8n"}
     out = []
     for e in lscomp.tune_table():
         if e["kind"] not in kinds:

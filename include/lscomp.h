@@ -245,8 +245,10 @@ int lscomp_plan_destroy(lscomp_plan *plan);
 
 /* Launch-configuration tuner (no counterpart in the reference, whose launch
    shape is fixed).  A configuration is the encoder CTA shape (2 groups of 8,
-   7 or -- single stacks -- 13 compute warps) and the most 8x8 blocks a tile holds (uint16: 256
-   or 128; uint32: 128 or 64); the decoder only has the tile size.  Every
+   7 or -- single stacks -- 13 compute warps; for lossless uint16 single
+   stacks also 2 x 8 with shorter code paths for small values) and the most
+   8x8 blocks a tile holds (uint16: 256 or 128; uint32: 128 or 64); the
+   decoder only has the tile size.  Every
    configuration writes the same stream.  With tuning on (the default;
    environment LSCOMP_AUTOTUNE=0 or lscomp_tune_mode(0) turns it off) the
    first compress / decompress / batch call of a key -- element type, bins
@@ -262,7 +264,8 @@ int lscomp_plan_destroy(lscomp_plan *plan);
    previous mode.  lscomp_tune_report writes the table as text (one line per
    key: "es layout pool kind vec bzb -> shape tile_blocks", then
    " | shape tile_blocks ms" per timed candidate; kind 0 compress, 1 batch,
-   2 decompress; shape -1 = rule, 0 = 2x8, 1 = 2x7, 2 = 2x13) and returns the bytes
+   2 decompress; shape -1 = rule, 0 = 2x8, 1 = 2x7, 2 = 2x13, 3 = 2x8 with
+   the short paths) and returns the bytes
    needed including the terminating NUL.  lscomp_tune_save / _load write and
    read that text (load replaces the keys it names; a malformed file changes
    nothing and returns LSCOMP_ERR_ARG).  Single stacks of fewer than 4

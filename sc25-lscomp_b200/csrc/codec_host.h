@@ -199,10 +199,10 @@ inline int ctas_per_sm(K kernel, size_t smem)
     return n > 0 ? n : 1;
 }
 
-template <typename T, int VEC, int BINS, bool POOL, int GRP, int WPG, bool BATCH>
+template <typename T, int VEC, int BINS, bool POOL, int GRP, int WPG, bool BATCH, bool NARROW = false>
 inline int launch_enc_w(const EncArgs<T> &a, int sm_count, cudaStream_t st)
 {
-    auto k = enc_kernel<T, VEC, BINS, POOL, GRP, WPG, BATCH>;
+    auto k = enc_kernel<T, VEC, BINS, POOL, GRP, WPG, BATCH, NARROW>;
     const size_t smem = sizeof(EncSmem);
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     // persistent: one CTA per SM (the CTA holds ~200 KB of rings)
@@ -235,7 +235,12 @@ inline double unit_fill(const Geom &g, uint32_t wpg)
 // units keep 8).  Groups of 13 keep only the header bytes between the two
 // passes and read the rows again from the input slot (72 registers a
 // thread, 28 compute warps on the SM).  shape 0 / 1 / 2 force 2 x 8 / 2 x 7
-// / 2 x 13 (uint16; 2 x 13 for single stacks only; uint32 always runs 2 x 8).
+// / 2 x 13 (uint16; 2 x 13 for single stacks only; uint32 always runs 2 x 8);
+// shape 3 is 2 x 8 with block_pack's short paths for small values, for
+// lossless uint16 single stacks only (a tuner candidate, never a rule: it
+// gains where nearly every unit takes a short path, XPCS-like data, and
+// loses a little elsewhere, where its four unrolled copies of the longer
+// unit code crowd the instruction cache).
 constexpr int kWideWpg = 13;
 
 template <typename T, int VEC, int BINS, bool POOL, bool BATCH>
@@ -249,6 +254,8 @@ inline int launch_enc_t(const EncArgs<T> &a, int shape, int sm_count, cudaStream
         }
         if constexpr (!BATCH)
             if (shape == 2) return launch_enc_w<T, VEC, BINS, POOL, 2, kWideWpg, BATCH>(a, sm_count, st);
+        if constexpr (!BATCH && BINS == BINS_IDENT)
+            if (shape == 3) return launch_enc_w<T, VEC, BINS, POOL, 2, 8, BATCH, true>(a, sm_count, st);
         if (shape == 1) return launch_enc_w<T, VEC, BINS, POOL, 2, 7, BATCH>(a, sm_count, st);
     }
     return launch_enc_w<T, VEC, BINS, POOL, LSC_ENC_GROUPS, LSC_ENC_WPG, BATCH>(a, sm_count, st);
@@ -333,7 +340,7 @@ struct TuneKey {
 int tune_mode();  // 1: tune keys not in the table on first use
 bool tune_lookup(const TuneKey &k, TuneCfg &c);  // counts a hit when found
 void tune_store(const TuneKey &k, const TuneCfg &c, const std::vector<std::pair<TuneCfg, float>> &times);
-std::vector<TuneCfg> tune_candidates(int es, int kind);
+std::vector<TuneCfg> tune_candidates(int es, int kind, int layout);
 
 constexpr int kTuneReps = 3;
 // Single stacks of fewer tiles than this many per SM are not tuned (their
@@ -364,7 +371,7 @@ inline TuneCfg tune_choose(lscomp_workspace *ws, const TuneKey &key, const TuneC
     }
     std::vector<std::pair<TuneCfg, float>> times;
     bool ok = true;
-    for (const TuneCfg &cand : tune_candidates(key.es, key.kind)) {
+    for (const TuneCfg &cand : tune_candidates(key.es, key.kind, key.layout)) {
         ok = run(cand) == LSCOMP_OK && read_ctl(ws, st) == LSCOMP_OK;
         if (ok) ok = cudaEventRecord(e0, st) == cudaSuccess;
         for (int i = 0; ok && i < kTuneReps; i++) ok = run(cand) == LSCOMP_OK;

@@ -1178,8 +1178,9 @@ __device__ __forceinline__ void block_pack(const Row<T> &A0, const Row<T> &B0, u
 // and the dependent steps of one tile (reductions, scan, barriers) overlap
 // with another's.  Per tile: pass A from the input ring into registers and
 // header bytes, tile scan and aggregate publication, pass B into the
-// payload ring.
-template <typename T, int VEC, int BINS, bool POOL, int GRP, int WPG, bool BATCH>
+// payload ring.  NARROW: the unrolled (register-resident) shapes also take
+// block_pack's short paths for small values (the RELOAD shapes always do).
+template <typename T, int VEC, int BINS, bool POOL, int GRP, int WPG, bool BATCH, bool NARROW>
 __device__ __forceinline__ void enc_compute(const EncArgs<T> &a, EncSmem &sm)
 {
     constexpr int UMAX = (Elem<T>::kTileBlocks / 8 + WPG - 1) / WPG;  // units per warp per tile
@@ -1312,7 +1313,7 @@ __device__ __forceinline__ void enc_compute(const EncArgs<T> &a, EncSmem &sm)
                 if (u < nunits) {
                     const uint32_t b = u * 8 + jb;
                     const bool active = b < ti.nblk;
-                    block_pack<T, BINS == BINS_IDENT, false>(A[q], B[q], hq[q], active, r, xs, cB,
+                    block_pack<T, BINS == BINS_IDENT, NARROW>(A[q], B[q], hq[q], active, r, xs, cB,
                                                              st + (active ? off[b] : 0u));
                 }
             }
@@ -1486,7 +1487,7 @@ __device__ __forceinline__ void enc_writer(const EncArgs<T> &a, EncSmem &sm, uin
     }
 }
 
-template <typename T, int VEC, int BINS, bool POOL, int GRP, int WPG, bool BATCH>
+template <typename T, int VEC, int BINS, bool POOL, int GRP, int WPG, bool BATCH, bool NARROW = false>
 __global__ void __launch_bounds__(EncShape<GRP, WPG>::kThreads, 1) enc_kernel(const EncArgs<T> a)
 {
     using S = EncShape<GRP, WPG>;
@@ -1512,7 +1513,7 @@ __global__ void __launch_bounds__(EncShape<GRP, WPG>::kThreads, 1) enc_kernel(co
     }
     __syncthreads();
     if (warp < (uint32_t)S::kCompute)
-        enc_compute<T, VEC, BINS, POOL, GRP, WPG, BATCH>(a, sm);
+        enc_compute<T, VEC, BINS, POOL, GRP, WPG, BATCH, NARROW>(a, sm);
     else if (warp == (uint32_t)S::kProducerWarp)
         enc_producer<T, GRP, BATCH>(a, sm);
     else

@@ -53,9 +53,11 @@ bool valid_cfg(const TuneKey &k, const TuneCfg &c)
 {
     const uint32_t maxb = k.es == 2 ? 256u : 128u;
     if (c.tile_blocks < 8 || c.tile_blocks > maxb || c.tile_blocks % 8) return false;
-    if (c.shape < -1 || c.shape > 2) return false;
+    if (c.shape < -1 || c.shape > 3) return false;
     if (c.shape >= 1 && k.es != 2) return false;
     if (c.shape == 2 && k.kind == kTuneBatch) return false;  // 2 x 13 runs single stacks only
+    // 2 x 8 with the short paths: lossless single-stack compression only
+    if (c.shape == 3 && (k.kind != kTuneCompress || k.layout != BINS_IDENT)) return false;
     if (k.vec != 16 && k.vec != 4 && !(k.vec == 2 && k.es == 2)) return false;
     return k.es == 2 || k.es == 4;
 }
@@ -99,11 +101,12 @@ void tune_store(const TuneKey &k, const TuneCfg &c, const std::vector<std::pair<
     e.times = times;
 }
 
-// Candidates per element size and call kind.  Encoder: CTA shape 2 x 8,
-// 2 x 7 or (single stacks) 2 x 13 warps (uint16) and tiles
-// of up to 256 or 128 blocks (uint16; 128 or 64 for uint32).  Decoder:
-// tiles of 256 or 128 (128 or 64) blocks.
-std::vector<TuneCfg> tune_candidates(int es, int kind)
+// Candidates per element size, call kind and bins layout.  Encoder: CTA
+// shape 2 x 8, 2 x 7 or (single stacks) 2 x 13 warps (uint16), and for
+// lossless uint16 single stacks 2 x 8 with the short paths for small values;
+// tiles of up to 256 or 128 blocks (uint16; 128 or 64 for uint32).
+// Decoder: tiles of 256 or 128 (128 or 64) blocks.
+std::vector<TuneCfg> tune_candidates(int es, int kind, int layout)
 {
     const uint32_t big = es == 2 ? 256u : 128u, small = big / 2;
     std::vector<TuneCfg> v;
@@ -115,6 +118,7 @@ std::vector<TuneCfg> tune_candidates(int es, int kind)
     v.push_back({0, big});
     if (es == 2) v.push_back({1, big});
     if (es == 2 && kind == kTuneCompress) v.push_back({2, big});
+    if (es == 2 && kind == kTuneCompress && layout == BINS_IDENT) v.push_back({3, big});
     v.push_back({0, small});
     if (es == 2) v.push_back({1, small});
     return v;

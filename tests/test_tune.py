@@ -67,13 +67,19 @@ def test_table_roundtrip(lzc, tmp_path):
                     "4 1 1 0 2 9 -> 0 64\n", "2 1 1 0 8 9 -> 0 64\n",
                     "2 1 1 1 16 0 -> 2 256\n",   # 2 x 13 runs single stacks only
                     "4 1 1 0 16 9 -> 2 128\n",   # and uint16 only
-                    "2 1 1 0 16 9 -> 3 256\n"):
+                    "2 1 1 0 16 9 -> 3 256\n",   # 2 x 8 with the short paths: lossless only,
+                    "2 3 0 1 16 0 -> 3 256\n",   # single stacks only,
+                    "4 3 0 0 16 9 -> 3 128\n",   # uint16 only
+                    "2 3 0 0 16 9 -> 4 256\n"):
             f.write_text("2 1 1 0 16 7 -> 0 8\n" + bad)
             with pytest.raises(lzc.LscompError):
                 lzc.tune_load(str(f))
             assert len(lzc.tune_table()) == 3
         with pytest.raises(lzc.LscompError):
             lzc.tune_load(str(tmp_path / "missing.txt"))
+        f.write_text("2 3 0 0 16 9 -> 3 256\n")  # lossless uint16 compress: accepted
+        lzc.tune_load(str(f))
+        assert len(lzc.tune_table()) == 4
     finally:
         lzc.tune_clear()
         lzc.tune_mode(prev)
@@ -123,6 +129,12 @@ def force(lz, tmp_path, line):
 
 
 CANDIDATES = {2: [(0, 256), (1, 256), (2, 256), (0, 128), (1, 128)], 4: [(0, 128), (0, 64)]}
+# lossless uint16 single stacks also try 2 x 8 with the short paths for small values
+CANDIDATES_LOSSLESS_U16 = [(0, 256), (1, 256), (2, 256), (3, 256), (0, 128), (1, 128)]
+
+
+def candidates(es, bins):
+    return CANDIDATES_LOSSLESS_U16 if es == 2 and all(x == 1 for x in bins) else CANDIDATES[es]
 DEC_CANDIDATES = {2: [(-1, 256), (-1, 128)], 4: [(-1, 128), (-1, 64)]}
 SHAPES = [(3, 37, 53), (2, 17, 2100), (4, 64, 1024), (2, 40, 1558), (1, 9, 2049)]
 
@@ -142,7 +154,7 @@ def test_every_config_same_stream(lz, ws, oracle, tmp_path, es, bins, p):
             d_in = to_dev(a)
             bzb = (dims[2] + 7) // 8
             key = f"{es} {layout_of(bins)} {pool_of(p)}"
-            for shape, tb in CANDIDATES[es]:
+            for shape, tb in candidates(es, bins):
                 force(lz, tmp_path, f"{key} 0 {vec_of(dims[2], es)} {bzb} -> {shape} {tb}")
                 hits = lz.tune_hits()
                 out = torch.full((lz.max_stream_bytes(dims, es),), 0xAB, dtype=torch.uint8, device="cuda")
