@@ -421,18 +421,24 @@ def bench_batch(args, local):
         config["subset"] = (f"the first {n} of {args.batch} stacks: their inputs and exact outputs fill the "
                             "free device memory")
 
-    def timed(fn, reps):
+    def timed(fn, reps, name=None):
+        # name: an NVTX range around the timed calls (not the warm-up), so a
+        # profiler can select exactly those launches (ncu --nvtx-include)
         for _ in range(max(args.warmup, 3)):
             fn()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ts = []
+        if name:
+            torch.cuda.nvtx.range_push(name)
         for _ in range(reps):
             e0.record(stream)
             fn()
             e1.record(stream)
             torch.cuda.synchronize()
             ts.append(e0.elapsed_time(e1))
+        if name:
+            torch.cuda.nvtx.range_pop()
         return float(np.median(ts))
 
     def fps(ms):
@@ -468,7 +474,7 @@ def bench_batch(args, local):
     t_batch = timed(lambda: lscomp.compress_batch_mixed(ws, items), args.steps)
     plan = lscomp.Plan(ws, items)
     assert plan.run() == got, "graph plan sizes differ from the batch call"
-    t_plan = timed(plan.run, args.steps)
+    t_plan = timed(plan.run, args.steps, "graph_plan")
     plan.close()
 
     def loop_stack():
@@ -503,7 +509,7 @@ def bench_batch(args, local):
         assert torch.equal(dchk[:ne], one), "batch decode differs from the single-stack decode"
     del dchk
     ditems = [(d_out, sl, dims, d_in, bins, p) for (d_in, dims, d_out, bins, p), (sl, _) in zip(items, got)]
-    t_dbatch = timed(lambda: lscomp.decompress_batch(ws, ditems), args.steps)
+    t_dbatch = timed(lambda: lscomp.decompress_batch(ws, ditems), args.steps, "batch_decompress")
 
     def loop_dstack():
         for d_s, sl, dims, d_o, bins, p in ditems:
