@@ -116,6 +116,19 @@ def random_stack(dims, seed, dtype=np.uint16, hi=60):
     return a
 
 
+def small_value_stack(dims, seed, dtype=np.uint16):
+    """Frames whose values stay below 4, 16, 128 and 300 in turn, so that the
+    short paths for small values (units of rate <= 2 and <= 4, quotients of
+    values below 128) and the longer ones all run; about half the values are
+    zero, so blocks also pool at p = 0.5."""
+    rng = np.random.default_rng(seed)
+    a = np.empty(dims, dtype=dtype)
+    for f in range(dims[0]):
+        a[f] = rng.integers(0, (4, 16, 128, 300)[f % 4], size=dims[1:])
+    a[rng.random(dims) < 0.55] = 0
+    return a
+
+
 def to_dev(a):
     view = np.int16 if a.dtype == np.uint16 else np.int32
     return torch.from_numpy(np.ascontiguousarray(a).view(view).ravel()).cuda()
@@ -137,18 +150,25 @@ def candidates(es, bins):
     return CANDIDATES_LOSSLESS_U16 if es == 2 and all(x == 1 for x in bins) else CANDIDATES[es]
 DEC_CANDIDATES = {2: [(-1, 256), (-1, 128)], 4: [(-1, 128), (-1, 64)]}
 SHAPES = [(3, 37, 53), (2, 17, 2100), (4, 64, 1024), (2, 40, 1558), (1, 9, 2049)]
+SMALL_SHAPES = [(4, 37, 53), (8, 40, 1558), (4, 64, 1024), (4, 17, 2100)]
 
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("es", [2, 4])
 @pytest.mark.parametrize("bins,p", [LOSSLESS, LOSSY, GENERAL])
-def test_every_config_same_stream(lz, ws, oracle, tmp_path, es, bins, p):
+@pytest.mark.parametrize("profile", ["wide", "small"])
+def test_every_config_same_stream(lz, ws, oracle, tmp_path, es, bins, p, profile):
+    if profile == "small" and es == 4:
+        pytest.skip("the short paths for small values are uint16 only")
     dtype = np.uint16 if es == 2 else np.uint32
     # each call must use the forced line (one table hit per call)
     prev = lz.tune_mode(1)
     try:
-        for i, dims in enumerate(SHAPES):
-            a = random_stack(dims, seed=100 + i, dtype=dtype)
+        for i, dims in enumerate(SHAPES if profile == "wide" else SMALL_SHAPES):
+            if profile == "wide":
+                a = random_stack(dims, seed=100 + i, dtype=dtype)
+            else:
+                a = small_value_stack(dims, seed=200 + i, dtype=dtype)
             s_o, rs_o = oracle.compress(a, dims, bins, p, dtype=dtype)
             d_o = oracle.decompress(s_o, dims, bins, p, dtype=dtype)
             d_in = to_dev(a)
