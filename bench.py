@@ -76,6 +76,9 @@ def parse():
                          "sweep of rates (its own JSON line)")
     ap.add_argument("--serve-seconds", type=float, default=60.0, help="duration of each rate of the serving run")
     ap.add_argument("--serve-max-mb", type=int, default=512, help="largest request of the serving benchmark")
+    ap.add_argument("--serve-pinned", action="store_true",
+                    help="serving benchmark: client buffers in page-locked host memory (copied by the device "
+                         "directly) instead of pageable numpy arrays (staged by the server's copy threads)")
     ap.add_argument("--serve-arena-gb", type=int, default=120,
                     help="device arena of the serving benchmark's server (its admission cap)")
     ap.add_argument("--batch-frames", type=int, default=64, help="largest frame count of a batch stack")
@@ -554,8 +557,21 @@ def bench_serve(args, local):
     (256 KB .. --serve-max-mb of 1024x1024 or 1813x1558 uint16 frames), 70%
     compress / 30% decompress, 60% lossless / 40% lossy (-b 3 5 10 15
     -p 0.5), host buffers in and out.  Latency = queue + service time per
-    request."""
+    request.  --serve-pinned puts every client buffer in page-locked host
+    memory, which the server copies directly; otherwise the buffers are
+    pageable and go through its staging."""
+    import torch
+
     import lscomp
+
+    def client(a):
+        # a client buffer equal to a: pageable numpy, or a numpy view of a
+        # page-locked tensor (which it keeps alive)
+        if not args.serve_pinned:
+            return a
+        v = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True).numpy().view(a.dtype).reshape(a.shape)
+        v[...] = a
+        return v
 
     rng = np.random.default_rng(5)
     pool = []
@@ -568,7 +584,7 @@ def bench_serve(args, local):
             h = max(8, int(size / (2 * w)))
         dims = (frames, h, w)
         kind = "xpcs" if i % 2 else "cssi"
-        pool.append((dims, getattr(lscomp, f"synth_{kind}")(dims, seed=100 + i).reshape(dims)))
+        pool.append((dims, client(getattr(lscomp, f"synth_{kind}")(dims, seed=100 + i).reshape(dims))))
     modes = [("lossless", (1, 1, 1, 1), 1.0), ("lossy", (3, 5, 10, 15), 0.5)]
     arena = int(args.serve_arena_gb) << 30
     srv = lscomp.Server(local, arena_bytes=arena)
@@ -578,13 +594,13 @@ def bench_serve(args, local):
         for name, bins, p in modes:
             o = np.zeros(64 + lscomp.max_stream_bytes(dims), dtype=np.uint8)
             r = srv.wait(srv.submit_compress(a, dims, bins, p, o))
-            conts[(k, name)] = o[: r["out_len"]].copy()
+            conts[(k, name)] = client(o[: r["out_len"]].copy())
     import queue as qmod
 
     # one output buffer per pool stack and direction, written before use, so
     # the run measures the server and not page faults on fresh client memory
     # (requests for the same stack may share one: their bytes are not checked)
-    outs = {k: (np.ones(64 + lscomp.max_stream_bytes(dims), dtype=np.uint8), np.ones_like(a))
+    outs = {k: (client(np.ones(64 + lscomp.max_stream_bytes(dims), dtype=np.uint8)), client(np.ones_like(a)))
             for k, (dims, a) in enumerate(pool)}
 
     def run_rate(rate, dur):
@@ -649,6 +665,8 @@ def bench_serve(args, local):
                                              "1024x1024 (XPCS-like) or 1813x1558 (CSSI-like) uint16 frames; 70/30 "
                                              "compress/decompress; 60/40 lossless/lossy", "arena_bytes": arena,
                                  "duration_s_per_rate": args.serve_seconds,
+                                 "client_buffers": "page-locked (direct copies)" if args.serve_pinned
+                                 else "pageable (staged through the server's pinned slots)",
                                  "copy_threads_per_direction": int(os.environ.get("LSCOMP_SERVER_COPY_THREADS", 8))}}))
 
 

@@ -335,7 +335,10 @@ int lscomp_decompress_container(lscomp_workspace *ws, const uint8_t *d_in, uint6
    request (a second waiter gets LSCOMP_ERR_ARG), and wait releases it.
    destroy runs what was submitted.  Environment: LSCOMP_SERVER_COPY_THREADS
    (default 8) host threads per direction copy between caller buffers and
-   staging. */
+   staging.  A caller buffer that is page-locked host memory (one
+   cudaHostAlloc / cudaHostRegister allocation, or a pinned tensor) is
+   copied to or from the device directly instead, with no staging and no
+   host-thread copy. */
 typedef struct lscomp_server lscomp_server;
 typedef struct lscomp_server_result {
     int status;          /* LSCOMP_OK or the request's error */

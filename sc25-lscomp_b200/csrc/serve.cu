@@ -28,7 +28,10 @@
 //
 // While one batch is on the GPU, later requests upload and earlier ones
 // download; the staging rings are a fixed 2 x 128 MB of pinned memory
-// whatever the arena's size.  A request's output depends only on the
+// whatever the arena's size.  A request whose host buffer is itself
+// page-locked (cudaHostAlloc, cudaHostRegister, or a framework's pinned
+// tensor) skips the staging ring in that direction: its bytes cross PCIe
+// with one direct copy, and no host thread copies them.  A request's output depends only on the
 // request: batched or alone, its container is byte-identical to what
 // lscomp_compress_container writes.
 #include <cuda_runtime.h>
@@ -63,6 +66,23 @@ uint64_t now_ns()
         .count();
 }
 
+// True when the first and the last byte of [p, p + n) are page-locked host
+// memory, so the device copies the range directly (a buffer is expected to
+// be one such allocation).  Pageable memory reports cudaMemoryTypeUnregistered.
+bool host_pinned(const void *p, uint64_t n)
+{
+    const uint8_t *b = static_cast<const uint8_t *>(p);
+    for (const uint8_t *q : {b, b + (n ? n - 1 : 0)}) {
+        cudaPointerAttributes a;
+        if (cudaPointerGetAttributes(&a, q) != cudaSuccess) {
+            cudaGetLastError();  // clear it: this query's error is not the caller's
+            return false;
+        }
+        if (a.type != cudaMemoryTypeHost) return false;
+    }
+    return true;
+}
+
 struct Request {
     int64_t id = 0;
     int op = 0;  // 0 compress, 1 decompress
@@ -83,6 +103,7 @@ struct Request {
     uint64_t out_len = 0;
     uint64_t t_submit = 0, t_start = 0, t_done = 0;
     bool done = false, waited = false;
+    bool in_pinned = false, out_pinned = false;  // host buffers the device can copy directly
     uint64_t footprint() const { return align_up(in_bytes) + align_up(out_dev); }
 };
 
@@ -231,6 +252,13 @@ void upload(lscomp_server *s, Request *r)
     uint8_t *dst = s->arena + r->in_off;
     static thread_local int next = 0;
     int st = LSCOMP_OK;
+    if (r->in_pinned) {  // one direct copy, no staging
+        if (cudaMemcpyAsync(dst, src, r->in_bytes, cudaMemcpyHostToDevice, s->up) != cudaSuccess)
+            st = LSCOMP_ERR_CUDA;
+        if (!st && cudaEventRecord(r->uploaded, s->up) != cudaSuccess) st = LSCOMP_ERR_CUDA;
+        r->status = st;
+        return;
+    }
     for (uint64_t o = 0; o < r->in_bytes; o += kSlotBytes) {
         const int k = next;
         next = (next + 1) % kSlots;
@@ -420,8 +448,13 @@ void launcher_main(lscomp_server *s)
 // ---------------------------------------------------------------- downloader
 // Device [src, src + n) to host dst through the ring: each slot's copy out
 // of staging runs while the following slots' device-to-host copies fly.
-int download(lscomp_server *s, uint8_t *dst, const uint8_t *src, uint64_t n)
+// A page-locked dst takes one direct copy instead.
+int download(lscomp_server *s, uint8_t *dst, const uint8_t *src, uint64_t n, bool pinned)
 {
+    if (pinned) {
+        if (n && cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, s->down) != cudaSuccess) return LSCOMP_ERR_CUDA;
+        return cudaStreamSynchronize(s->down) == cudaSuccess ? LSCOMP_OK : LSCOMP_ERR_CUDA;
+    }
     struct Piece {
         int k;
         uint64_t off, n;
@@ -466,9 +499,9 @@ void downloader_main(lscomp_server *s)
             uint8_t *out = static_cast<uint8_t *>(r->h_out);
             if (r->op == 0) {
                 memcpy(out, r->hdr, kHdr);
-                r->status = download(s, out + kHdr, s->arena + r->out_off, r->out_len - kHdr);
+                r->status = download(s, out + kHdr, s->arena + r->out_off, r->out_len - kHdr, r->out_pinned);
             } else {
-                r->status = download(s, out, s->arena + r->out_off, r->out_len);
+                r->status = download(s, out, s->arena + r->out_off, r->out_len, r->out_pinned);
             }
         }
         std::lock_guard<std::mutex> lk(s->mu);
@@ -600,6 +633,8 @@ int64_t lscomp_server_submit_compress(lscomp_server *s, uint32_t elem_bytes, con
     r->h_out = h_out;
     r->out_cap = out_cap;
     r->out_dev = elem_bytes == 2 ? lscomp_max_stream_bytes_u16(x, y, z) : lscomp_max_stream_bytes_u32(x, y, z);
+    r->in_pinned = host_pinned(h_in, r->in_bytes);
+    r->out_pinned = host_pinned(h_out, out_cap);
     return enqueue(s, r);
 }
 
@@ -626,6 +661,8 @@ int64_t lscomp_server_submit_decompress(lscomp_server *s, const void *h_containe
     r->h_out = h_out;
     r->out_cap = out_cap;
     r->out_dev = out_bytes;
+    r->in_pinned = host_pinned(h_container, r->in_bytes);
+    r->out_pinned = host_pinned(h_out, out_cap);
     return enqueue(s, r);
 }
 

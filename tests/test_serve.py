@@ -201,3 +201,60 @@ def test_second_waiter_refused(lz):
         t.join()
     assert sorted(got) == [-1, 0]
     srv.close()
+
+
+def pinned(a):
+    """A copy of a in page-locked host memory (a numpy view of a pinned
+    tensor, which the view keeps alive)."""
+    v = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True).numpy().view(a.dtype).reshape(a.shape)
+    v[...] = a
+    return v
+
+
+def test_pinned_buffers_direct(lz):
+    """Page-locked client buffers are copied by the device directly (no
+    staging): mixed with pageable ones in the same batches, every container
+    still equals the single-call container and every decode the input;
+    stacks larger than one staging slot (32 MB) included."""
+    reqs = requests(24, seed=7)
+    rng = np.random.default_rng(8)
+    big = rng.integers(0, 40, size=(24, 1024, 1024), dtype=np.uint16)  # 48 MB: more than one slot
+    reqs.append((big, big.shape, LOSSLESS[0], LOSSLESS[1]))
+    ws = lz.Workspace(0)
+    srv = lz.Server(0, arena_bytes=1 << 30)
+    ins, outs, ids = [], [], []
+    for i, (a, dims, bins, p) in enumerate(reqs):
+        pin_in, pin_out = i % 2 == 0, i % 3 != 1  # every combination of pinned and pageable
+        h_in = pinned(a) if pin_in else a
+        o = np.zeros(64 + lz.max_stream_bytes(dims, a.itemsize), dtype=np.uint8)
+        o = pinned(o) if pin_out else o
+        ins.append(h_in)
+        outs.append(o)
+        ids.append(srv.submit_compress(h_in, dims, bins, p, o))
+    res = [srv.wait(i) for i in ids]
+    conts = []
+    for (a, dims, bins, p), o, r in zip(reqs, outs, res):
+        assert r["status"] == 0
+        ref = alone(lz, ws, a, dims, bins, p)
+        assert r["out_len"] == len(ref)
+        assert np.array_equal(o[: r["out_len"]], ref)
+        conts.append(ref)
+    decs, ids = [], []
+    for i, ((a, dims, bins, p), c) in enumerate(zip(reqs, conts)):
+        c_in = pinned(c) if i % 3 == 0 else c
+        d = np.full(a.shape, 0xFF, dtype=a.dtype)
+        d = pinned(d) if i % 2 == 1 else d
+        decs.append((c_in, d))
+        ids.append(srv.submit_decompress(c_in, d))
+    for (a, dims, bins, p), (c_in, d), i in zip(reqs, decs, ids):
+        r = srv.wait(i)
+        assert r["status"] == 0
+        if bins == LOSSLESS[0]:
+            assert np.array_equal(d, a)
+        else:
+            view = np.int32 if a.itemsize == 4 else np.int16
+            cont = torch.from_numpy(np.array(c_in)).cuda()
+            ref = torch.empty(a.size, dtype=torch.int32 if a.itemsize == 4 else torch.int16, device="cuda")
+            lz.decompress_container(ws, cont, len(c_in), ref)
+            assert np.array_equal(d.view(view).ravel(), ref.cpu().numpy())
+    srv.close()
