@@ -20,8 +20,9 @@
 //     launches: the compress requests of one element type as one
 //     lscomp_compress_batch_ex_* launch (each stack with its own shape, bins
 //     and pooling threshold), the decompress requests of one element type as
-//     one lscomp_decompress_batch_*.  If a batch fails, its requests run
-//     again one at a time, so a bad request fails alone.
+//     one lscomp_decompress_batch_* (a group of one request runs the
+//     single-stack call instead).  If a batch fails, its requests run again
+//     one at a time, so a bad request fails alone.
 //   * downloader: streams each finished output back through its own ring of
 //     pinned slots, releases the request's arena space (which may admit the
 //     next waiting request) and completes the request.
@@ -343,6 +344,15 @@ void compress_group(lscomp_server *s, const std::vector<Request *> &v, uint32_t 
         pool[i] = r->p;
     }
     auto batch = [&](size_t i0, size_t cnt) {
+        if (cnt == 1) {
+            // one request: the single-stack kernel, which spares the batch
+            // launch's per-tile stack lookup (the same stream either way)
+            const lscomp_stack &q = stacks[i0];
+            return eb == 2 ? lscomp_compress_u16(s->ws, static_cast<const uint16_t *>(q.d_in), q.x, q.y, q.z,
+                                                 &bins[4 * i0], pool[i0], q.d_out, q.cap, &len[i0], &ref[i0], s->comp)
+                           : lscomp_compress_u32(s->ws, static_cast<const uint32_t *>(q.d_in), q.x, q.y, q.z,
+                                                 &bins[4 * i0], pool[i0], q.d_out, q.cap, &len[i0], &ref[i0], s->comp);
+        }
         return eb == 2 ? lscomp_compress_batch_ex_u16(s->ws, &stacks[i0], (uint32_t)cnt, &bins[4 * i0], &pool[i0],
                                                       &len[i0], &ref[i0], s->comp)
                        : lscomp_compress_batch_ex_u32(s->ws, &stacks[i0], (uint32_t)cnt, &bins[4 * i0], &pool[i0],
@@ -385,6 +395,14 @@ void decompress_group(lscomp_server *s, const std::vector<Request *> &v, uint32_
         pool[i] = r->p;
     }
     auto batch = [&](size_t i0, size_t cnt) {
+        if (cnt == 1) {  // one request: the single-stack decoder
+            const lscomp_stack &q = stacks[i0];
+            const uint8_t *in = static_cast<const uint8_t *>(q.d_in);
+            return eb == 2 ? lscomp_decompress_u16(s->ws, in, q.cap, q.x, q.y, q.z, &bins[4 * i0], pool[i0],
+                                                   reinterpret_cast<uint16_t *>(q.d_out), s->comp)
+                           : lscomp_decompress_u32(s->ws, in, q.cap, q.x, q.y, q.z, &bins[4 * i0], pool[i0],
+                                                   reinterpret_cast<uint32_t *>(q.d_out), s->comp);
+        }
         return eb == 2 ? lscomp_decompress_batch_u16(s->ws, &stacks[i0], (uint32_t)cnt, &bins[4 * i0], &pool[i0],
                                                      s->comp)
                        : lscomp_decompress_batch_u32(s->ws, &stacks[i0], (uint32_t)cnt, &bins[4 * i0], &pool[i0],
