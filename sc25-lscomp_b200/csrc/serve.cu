@@ -253,6 +253,9 @@ void upload(lscomp_server *s, Request *r)
     uint8_t *dst = s->arena + r->in_off;
     static thread_local int next = 0;
     int st = LSCOMP_OK;
+    // checked here, on the server's device, so that submitting makes no
+    // CUDA call on the client's thread
+    r->in_pinned = host_pinned(r->h_in, r->in_bytes);
     if (r->in_pinned) {  // one direct copy, no staging
         if (cudaMemcpyAsync(dst, src, r->in_bytes, cudaMemcpyHostToDevice, s->up) != cudaSuccess)
             st = LSCOMP_ERR_CUDA;
@@ -515,6 +518,7 @@ void downloader_main(lscomp_server *s)
         }
         if (!r->status) {
             uint8_t *out = static_cast<uint8_t *>(r->h_out);
+            r->out_pinned = host_pinned(out, r->out_cap);
             if (r->op == 0) {
                 memcpy(out, r->hdr, kHdr);
                 r->status = download(s, out + kHdr, s->arena + r->out_off, r->out_len - kHdr, r->out_pinned);
@@ -651,8 +655,6 @@ int64_t lscomp_server_submit_compress(lscomp_server *s, uint32_t elem_bytes, con
     r->h_out = h_out;
     r->out_cap = out_cap;
     r->out_dev = elem_bytes == 2 ? lscomp_max_stream_bytes_u16(x, y, z) : lscomp_max_stream_bytes_u32(x, y, z);
-    r->in_pinned = host_pinned(h_in, r->in_bytes);
-    r->out_pinned = host_pinned(h_out, out_cap);
     return enqueue(s, r);
 }
 
@@ -679,8 +681,6 @@ int64_t lscomp_server_submit_decompress(lscomp_server *s, const void *h_containe
     r->h_out = h_out;
     r->out_cap = out_cap;
     r->out_dev = out_bytes;
-    r->in_pinned = host_pinned(h_container, r->in_bytes);
-    r->out_pinned = host_pinned(h_out, out_cap);
     return enqueue(s, r);
 }
 
